@@ -1,0 +1,133 @@
+/* pfag.h — C ABI of the B200 time step of the multicellular phase-field /
+ * active-gel organoid model (drop-in for the step that
+ * main_code/run_with_active_gels.cpp:101-185 of the reference drives).
+ *
+ * Plain pointers and sizes only.  All state arrays use the reference layout:
+ * per-cell fields [Ntot][N_s][N_s] row-major (index n*N_s*N_s + i*N_s + j),
+ * shared fields [N_s][N_s].  The element type is double for a context created
+ * with precision 64 and float for precision 32; `const void *` arguments carry
+ * that type.  Every function returns PFAG_OK (0) or a negative PFAG_E* code;
+ * pfag_last_error() gives the message of the last failure on this thread.
+ */
+#ifndef PFAG_H
+#define PFAG_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    PFAG_OK = 0,
+    PFAG_E_ARG = -1,          /* invalid argument or parameter */
+    PFAG_E_CUDA = -2,         /* CUDA runtime / cuFFT failure */
+    PFAG_E_ZONE = -3,         /* a cell's zone or FFT box leaves the grid (the reference reads out of bounds there) */
+    PFAG_E_EMPTY_CELL = -4,   /* a cell has no site with phi > 0.5 (the reference divides by zero there) */
+    PFAG_E_UNSUPPORTED = -5,  /* configuration outside what the selected path supports */
+    PFAG_E_RELAX = -6         /* a reshaping loop passed rimax (the reference prints "Relaxation failure!" and goes on) */
+};
+
+/* Execution paths. */
+enum {
+    PFAG_PATH_PLAIN = 0,  /* one kernel per reference function, full-grid passes where the reference makes them, cuFFT */
+    PFAG_PATH_FUSED = 1   /* zone-restricted fused kernels, hand-written batched FFT, device-side convergence loops */
+};
+
+/* The parameter set of functions/constants_template.cpp:4-129 that the step
+ * reads (the same names; derived values already derived). */
+typedef struct pfag_params {
+    int N_s, Ntot, zone_size, N_current;
+    int rdev_threshold, rimax;
+    double dx, dt, R, s0, sigma, coupling_PF_AG;
+    double tau, alpha, beta, eta;
+    double tau_lum, beta_lum_cells, eta_lum_cells, xi_lum;
+    double alpha_ECM, tau_ECM, beta_ECM_cells, eta_ECM_cells, xi_ECM, beta_lum_ECM;
+    double wi, rtol, rdt, friction;
+    double a_tan_apical, a_tan_basal, a_tan_lateral;
+    double a_ort_apical, a_ort_basal, a_ort_lateral;
+    double b_ap, b_bas, b_lat;
+    double matgenrate_apical, matgenrate_basal, matgenrate_lateral;
+    double degrate_apical, degrate_basal, degrate_lateral;
+    double viscosity_ap, viscosity_bas, viscosity_lat;
+} pfag_params;
+
+/* Per-step diagnostics of the last pfag_step call (its final step). */
+typedef struct pfag_stats {
+    int cell_iters_max;     /* largest reshaping iteration count over cells (cell_phase_functions.cpp:475-574) */
+    int cell_iters_sum;     /* sum over cells */
+    int lum_iters;          /* lumen reshaping iterations (cell_phase_functions.cpp:774-869, side 0) */
+    int ecm_iters;          /* ECM reshaping iterations (side 1) */
+    int relax_failures;     /* loops that passed rimax */
+    double sum_ecm;         /* sum of h(ECM) dx^2 (cell_phase_functions.cpp:376-386) */
+} pfag_stats;
+
+typedef struct pfag_ctx pfag_ctx;
+
+const char *pfag_last_error(void);
+int pfag_version(void);
+
+/* Create a context on the current CUDA device; allocates the device state.
+ * precision: 64 (double) or 32 (float).  path: PFAG_PATH_*. */
+int pfag_create(const pfag_params *p, int precision, int path, pfag_ctx **out);
+int pfag_destroy(pfag_ctx *ctx);
+
+/* Host -> device state (run_with_active_gels.cpp:65-75 then :92-98):
+ * phi, rho [Ntot][N][N], lum, ECM [N][N]; phin, rhon, hfunc_cell start at zero
+ * and are then set to phi, rho (the copies at :92-98).  Synchronous. */
+int pfag_upload(pfag_ctx *ctx, const void *phi, const void *rho, const void *lum, const void *ecm);
+/* Device -> host state; any pointer may be NULL.  Synchronous. */
+int pfag_download(pfag_ctx *ctx, void *phi, void *rho, void *lum, void *ecm);
+
+/* Advance nsteps steps from step index it0 (the loop body of
+ * run_with_active_gels.cpp:110-184 without the snapshot).  Synchronous. */
+int pfag_step(pfag_ctx *ctx, int it0, int nsteps);
+/* The same, enqueued on the context's stream without a final synchronisation
+ * (device-resident benchmarking); errors surface at the next synchronous call. */
+int pfag_step_async(pfag_ctx *ctx, int it0, int nsteps);
+int pfag_sync(pfag_ctx *ctx);
+
+/* Observables of the last step: s (Ntot doubles, cell areas), xc, yc (Ntot ints). */
+int pfag_get_areas(pfag_ctx *ctx, double *s, double *f0);
+int pfag_get_centres(pfag_ctx *ctx, int *xc, int *yc);
+int pfag_get_stats(pfag_ctx *ctx, pfag_stats *st);
+/* Per-cell reshaping iteration counts of the last step (Ntot ints). */
+int pfag_get_cell_iters(pfag_ctx *ctx, int *iters);
+/* Per-cell velocity of the last step's spectral solve, Re(IFFT(v))/M^2 on the
+ * FFT box (rho_functions.cpp:449-456): vx, vy [Ntot][M][M], M = 2*zone_size-2.
+ * Requires pfag_set_debug(ctx, 1) before the step. */
+int pfag_set_debug(pfag_ctx *ctx, int flags);
+int pfag_get_velocity(pfag_ctx *ctx, void *vx, void *vy);
+
+/* Device pointers of the state (phi, rho: [Ntot][N][N]; lum, ECM: [N][N]). */
+int pfag_device_state(pfag_ctx *ctx, void **phi, void **rho, void **lum, void **ecm);
+/* CUDA stream (cudaStream_t) the context enqueues on. */
+void *pfag_stream(pfag_ctx *ctx);
+/* Number of kernel launches the last pfag_step / pfag_step_async enqueued. */
+long pfag_launch_count(pfag_ctx *ctx);
+
+/* ---- One entry point per reference function on the step path. ----------
+ * Each operates on the context's device state, exactly as the reference
+ * function of the same name does on its OpenACC-present arrays.  They are
+ * what the C++ drop-in layer (reference signatures) forwards to. */
+int pfag_fn_find_centres_cells(pfag_ctx *ctx);                 /* useful_functions.cpp:193-227 */
+int pfag_fn_create_turnover_rates_tensions(pfag_ctx *ctx);     /* rho_functions.cpp:286-405 */
+int pfag_fn_compute_hfunc_3d_tables_kernels_loop_n(pfag_ctx *ctx); /* useful_functions.cpp:233-251 */
+int pfag_fn_compute_all_hfunc_2d_tables_kernels(pfag_ctx *ctx);   /* useful_functions.cpp:272-285 */
+int pfag_fn_compute_normal_grad_phi(pfag_ctx *ctx);            /* useful_functions.cpp:326-354 + :391-420 */
+int pfag_fn_compute_prod_norm_delta(pfag_ctx *ctx);            /* rho_functions.cpp:13-30 */
+int pfag_fn_compute_psi_kernels(pfag_ctx *ctx);                /* useful_functions.cpp:305-322 */
+int pfag_fn_sum_s_kernels(pfag_ctx *ctx, double *s_host, double *f0_host); /* useful_functions.cpp:168-190 */
+int pfag_fn_update_all_cortices(pfag_ctx *ctx);                /* rho_functions.cpp:409-471 */
+int pfag_fn_update_lumen_and_ECM(pfag_ctx *ctx);               /* cell_phase_functions.cpp:372-444 + useful_functions.cpp:439-462 */
+int pfag_fn_reshaping_lumen_or_ECM(pfag_ctx *ctx, int which);  /* cell_phase_functions.cpp:709-871; which 0 lumen, 1 ECM */
+int pfag_fn_compute_normal_to_phi(pfag_ctx *ctx);              /* useful_functions.cpp:356-388 + :391-420 */
+int pfag_fn_update_all_cells(pfag_ctx *ctx);                   /* cell_phase_functions.cpp:126-217 + useful_functions.cpp:391-420 */
+int pfag_fn_reshaping_cells(pfag_ctx *ctx);                    /* cell_phase_functions.cpp:447-580 */
+int pfag_fn_copy_back(pfag_ctx *ctx);                          /* run_with_active_gels.cpp:175-182 */
+/* saving_out_functions (useful_functions.cpp:66-99): device state -> host
+ * snapshot slot; phi_out/rho_out get Ntot*N*N, lum_out/ecm_out N*N elements. */
+int pfag_fn_saving_out_functions(pfag_ctx *ctx, void *phi_out, void *rho_out, void *lum_out, void *ecm_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
