@@ -97,6 +97,11 @@ int pfag_get_cell_iters(pfag_ctx *ctx, int *iters);
 int pfag_set_debug(pfag_ctx *ctx, int flags);
 int pfag_get_velocity(pfag_ctx *ctx, void *vx, void *vy);
 
+/* Bound on the device-side relaxation loops of the fused path (default
+ * rimax + 2, the bound the reference's loops have).  A loop that reaches the
+ * cap stops with PFAG_E_RELAX reported at the next synchronisation. */
+int pfag_set_relax_cap(pfag_ctx *ctx, int cap);
+
 /* Device pointers of the state (phi, rho: [Ntot][N][N]; lum, ECM: [N][N]). */
 int pfag_device_state(pfag_ctx *ctx, void **phi, void **rho, void **lum, void **ecm);
 /* CUDA stream (cudaStream_t) the context enqueues on. */

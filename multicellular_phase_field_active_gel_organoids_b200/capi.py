@@ -55,7 +55,7 @@ _lib = None
 EXPORTS = [
     "pfag_last_error", "pfag_version", "pfag_create", "pfag_destroy", "pfag_upload", "pfag_download",
     "pfag_step", "pfag_step_async", "pfag_sync", "pfag_get_areas", "pfag_get_centres", "pfag_get_stats",
-    "pfag_get_cell_iters", "pfag_set_debug", "pfag_get_velocity", "pfag_device_state", "pfag_stream", "pfag_launch_count",
+    "pfag_get_cell_iters", "pfag_set_relax_cap", "pfag_set_debug", "pfag_get_velocity", "pfag_device_state", "pfag_stream", "pfag_launch_count",
     "pfag_fn_find_centres_cells", "pfag_fn_create_turnover_rates_tensions",
     "pfag_fn_compute_hfunc_3d_tables_kernels_loop_n", "pfag_fn_compute_all_hfunc_2d_tables_kernels",
     "pfag_fn_compute_normal_grad_phi", "pfag_fn_compute_prod_norm_delta", "pfag_fn_compute_psi_kernels",
@@ -86,6 +86,7 @@ def lib() -> ctypes.CDLL:
         L.pfag_get_stats.argtypes = [vp, ctypes.POINTER(PfagStats)]
         L.pfag_set_debug.argtypes = [vp, ctypes.c_int]
         L.pfag_get_cell_iters.argtypes = [vp, vp]
+        L.pfag_set_relax_cap.argtypes = [vp, ctypes.c_int]
         L.pfag_get_velocity.argtypes = [vp, vp, vp]
         L.pfag_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
                                         ctypes.POINTER(vp)]
@@ -205,6 +206,9 @@ class Simulation:
         it = np.empty(self.ncells, np.int32)
         check(lib().pfag_get_cell_iters(self.h, _ptr(it)))
         return it
+
+    def set_relax_cap(self, cap: int):
+        check(lib().pfag_set_relax_cap(self.h, int(cap)))
 
     def set_debug(self, flags: int = 1):
         check(lib().pfag_set_debug(self.h, int(flags)))

@@ -97,6 +97,7 @@ extern "C" int pfag_create(const pfag_params *p, int precision, int path, pfag_c
     c->prec = precision;
     c->path = path;
     c->rsz = precision == 64 ? 8 : 4;
+    c->relax_cap = p->rimax + 2;
     c->N = p->N_s; c->Ntot = p->Ntot; c->zone = p->zone_size; c->M = 2 * p->zone_size - 2;
     c->ng = (size_t)c->N * c->N;
     c->nc = (size_t)c->Ntot * c->ng;
@@ -250,6 +251,12 @@ extern "C" int pfag_get_centres(pfag_ctx *c, int *xc, int *yc) {
 extern "C" int pfag_get_stats(pfag_ctx *c, pfag_stats *st) {
     if (!c || !st) return PFAG_E_ARG;
     *st = c->stats;
+    return PFAG_OK;
+}
+
+extern "C" int pfag_set_relax_cap(pfag_ctx *c, int cap) {
+    if (!c || cap < 1) { pfag_set_error("relax cap must be >= 1"); return PFAG_E_ARG; }
+    c->relax_cap = cap;
     return PFAG_OK;
 }
 

@@ -101,6 +101,7 @@ struct pfag_ctx {
     pfag_stats stats;
     long launches;
     int debug;
+    int relax_cap;        // device-side loop bound (fused path)
     void *d_vx, *d_vy;
     // fused-path resources (opaque, owned by pfag_fused.cu)
     void *fused;

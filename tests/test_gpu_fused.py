@@ -1,0 +1,70 @@
+"""Fused path (zone-restricted kernels, hand-written FFT, persistent relaxation
+loops) against the reference's own FP64 run and against the plain path.
+FP64 tolerances: relative L-inf 1e-9 on phi, rho, lumen, ECM and velocity,
+areas 1e-10, centres exact.  FP32 (FP64 islands for areas and loop sums):
+per-cell area 1e-4 against the FP64 reference."""
+import numpy as np
+import pytest
+
+from multicellular_phase_field_active_gel_organoids_b200 import capi
+from multicellular_phase_field_active_gel_organoids_b200.params import CONFIGS
+from oracle import refrun
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_linf(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def run_gpu(cfg, nsteps, precision, path, velocity=False):
+    dtype = np.float64 if precision == 64 else np.float32
+    with capi.Simulation(cfg.params(), precision, path) as sim:
+        sim.set_relax_cap(100000)
+        sim.upload(*cfg.initial_state(dtype))
+        if velocity:
+            sim.set_debug(1)
+        sim.step(0, nsteps)
+        phi, rho, lum, ecm = sim.download()
+        out = dict(phi=phi, rho=rho, lum=lum, ECM=ecm, s=sim.areas()[0], xc=sim.centres()[0],
+                   yc=sim.centres()[1], iters=sim.cell_iters(), stats=sim.stats())
+        if velocity:
+            out["velocity"] = sim.velocity()
+    return out
+
+
+@pytest.fixture(scope="module")
+def tiny_ref():
+    cfg = CONFIGS["tiny"]()
+    return cfg, refrun.run_reference(cfg.params(), cfg.initial_state(), 5, velocity=True)
+
+
+def test_fused_fp64_tiny_matches_reference(tiny_ref):
+    cfg, ref = tiny_ref
+    got = run_gpu(cfg, 5, 64, capi.PATH_FUSED, velocity=True)
+    assert np.array_equal(got["xc"], ref["xc"]) and np.array_equal(got["yc"], ref["yc"])
+    errs = {k: rel_linf(got[k], ref[k]) for k in ("phi", "rho", "lum", "ECM", "s")}
+    assert all(errs[k] <= 1e-9 for k in ("phi", "rho", "lum", "ECM")), errs
+    assert errs["s"] <= 1e-10, errs
+    vx, vy = got["velocity"]
+    rvx, rvy = ref["velocity"]
+    assert rel_linf(vx, rvx) <= 1e-9 and rel_linf(vy, rvy) <= 1e-9
+
+
+def test_fused_fp32_tiny_area(tiny_ref):
+    cfg, ref = tiny_ref
+    got = run_gpu(cfg, 5, 32, capi.PATH_FUSED)
+    assert np.array_equal(got["xc"], ref["xc"])
+    assert rel_linf(got["s"], ref["s"]) <= 1e-4
+
+
+def test_fused_vs_plain_cfg0_fp64():
+    cfg = CONFIGS["cfg0"]()
+    a = run_gpu(cfg, 4, 64, capi.PATH_FUSED)
+    b = run_gpu(cfg, 4, 64, capi.PATH_PLAIN)
+    assert np.array_equal(a["iters"], b["iters"])
+    for k in ("phi", "rho", "lum", "ECM"):
+        assert rel_linf(a[k], b[k]) <= 1e-9, (k, rel_linf(a[k], b[k]))
+    assert rel_linf(a["s"], b["s"]) <= 1e-10
