@@ -1,0 +1,448 @@
+#!/usr/bin/env python3
+"""Benchmark of the organoid time step on B200 (one process per GPU).
+
+Workload: the 1024x1024, 64-cell organoid (zone_size 129, FFT box 256), the
+reference's step (main_code/run_with_active_gels.cpp:101-185) advanced by the
+fused path.  Metric: site-updates/s = Ntot * N_s^2 cell-grid sites per step,
+whole job.  Each GPU advances its own organoid replica (the step shards by
+cell only with a psi all-reduce; replicas are what runs here), so scaling is
+weak.  Between timed steps L2 is flushed by writing a 256 MiB buffer; each
+step is timed with CUDA events on the context's stream.
+
+  python bench.py --gpus N --steps K --warmup W            # this framework
+  python bench.py --impl reference --steps K --warmup W    # reference on the host cores
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "site-updates/s/B200 (cells x grid x steps), fast vs plain FP64 at stated error"
+UNIT = "site-updates/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
+    ap.add_argument("--config", default="cfg1")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true")
+    return ap.parse_args()
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return ws, rank, local
+
+
+class Dist:
+    """Barrier and max-over-ranks of scalars (torch.distributed only when N > 1)."""
+
+    def __init__(self, ws, rank, local, backend):
+        self.ws, self.rank = ws, rank
+        self.td = None
+        if ws > 1:
+            import datetime
+            import torch
+            import torch.distributed as td
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+            td.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+            self.td, self.torch, self.backend = td, torch, backend
+
+    def barrier(self):
+        if self.td:
+            self.td.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.td:
+            return x
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=dev)
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.td:
+            return x
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=dev)
+        self.td.all_reduce(t, op=self.td.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.td:
+            self.td.barrier()
+            self.td.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms in the background."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self) -> dict:
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for k, nm in enumerate(names[1:], start=5):
+                    if r[k].lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+def kernel_bytes(cfg, precision: int, iters: dict) -> dict:
+    """Algorithmic bytes per launch of the fused kernels (compulsory traffic:
+    each array element the kernel must read or write once)."""
+    w = precision // 8
+    n, N, z = cfg.ncells, cfg.N, cfg.zone_size
+    M, Wz = cfg.box, 2 * z + 2
+    box = n * M * M
+    zone = n * (2 * z) * (2 * z)
+    ring = n * Wz * Wz
+    out = {
+        # reads phi (centre), phi_{n-1}, phi_{n+1}, rho, lum, ECM; writes pi_xx+i pi_yy, pi_xy, R, class byte
+        "kf_boxA": box * (6 * w + 5 * w + 1),
+        "kf_boxB": box * (4 * w + 1 + 2 * w),
+        "kf_boxC": box * (2 * w + w + 2 * w),
+        "kf_boxD": box * (2 * w + 2 * w),
+        "kf_boxE": box * (2 * w + w + w + w),
+        # reads phi, rho, hfunc, psi, h(lum), h(ECM); writes phin, J_x, J_y
+        "kf_update": ring * 9 * w,
+        # per iteration: read P and J (x, y), write Q, over each active cell's zone
+        "kf_reshape": (2 * z) * (2 * z) * 4 * w * max(iters.get("cell_iters_sum", n), 1),
+        "kf_psi": N * N * (2 * w + 3 * w) + zone * w,
+        "kf_hfunc_area": zone * 2 * w,
+        "kf_centroid": zone * w,
+        "kf_rho_copy": box * 2 * w,
+        # update (read lum, ECM, psi, h's, write lumn, ECMn), normals (read 4, write 4),
+        # per relaxation iteration (read P, Jx, Jy, write Q) for each field
+        "kf_lum": N * N * w * (7 + 8 + 4 * max(iters.get("lum_iters", 1) + iters.get("ecm_iters", 1), 1)),
+    }
+    return out
+
+
+def run_ours(args, ws, rank, local, dist: Dist):
+    from multicellular_phase_field_active_gel_organoids_b200 import capi
+    from multicellular_phase_field_active_gel_organoids_b200.params import CONFIGS
+
+    capi.lib()   # loads libpfag.so and, with it, the CUDA runtime the library uses
+    rt = ctypes.CDLL("libcudart.so.12")
+    if rt.cudaSetDevice(local) != 0:
+        raise RuntimeError(f"cudaSetDevice({local}) failed")
+    cfg = CONFIGS[args.config]()
+    p = cfg.params()
+    prec = args.precision
+    dtype = np.float64 if prec == 64 else np.float32
+    sites = cfg.ncells * cfg.N * cfg.N
+    init = cfg.initial_state(dtype)
+
+    # L2 flush buffer and events through the CUDA runtime (no torch on the step path)
+    flush = ctypes.c_void_p()
+    assert rt.cudaMalloc(ctypes.byref(flush), ctypes.c_size_t(L2_FLUSH_BYTES)) == 0
+    rt.cudaEventCreate.argtypes = [ctypes.POINTER(ctypes.c_void_p)]
+    rt.cudaEventRecord.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    rt.cudaEventSynchronize.argtypes = [ctypes.c_void_p]
+    rt.cudaEventElapsedTime.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_void_p, ctypes.c_void_p]
+    rt.cudaMemsetAsync.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p]
+    rt.cudaStreamSynchronize.argtypes = [ctypes.c_void_p]
+
+    sim = capi.Simulation(p, prec, capi.PATH_FUSED)
+    sim.upload(*init)
+    stream = ctypes.c_void_p(sim.stream())
+    nev = args.steps
+    ev0 = [ctypes.c_void_p() for _ in range(nev)]
+    ev1 = [ctypes.c_void_p() for _ in range(nev)]
+    for e in ev0 + ev1:
+        rt.cudaEventCreate(ctypes.byref(e))
+    # warm-up (W >= 3 untimed steps)
+    it = 0
+    for _ in range(max(args.warmup, 3)):
+        sim.step(it, 1)
+        it += 1
+    capi.check(capi.lib().pfag_set_profile(sim.h, 1))
+    capi.lib().pfag_profile_read(sim.h, None, None, None, 0)   # clear
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    dist.barrier()
+    rt.cudaStreamSynchronize(stream)
+    launches = 0
+    t_wall0 = time.perf_counter()
+    for k in range(nev):
+        rt.cudaMemsetAsync(flush, k & 0xff, L2_FLUSH_BYTES, stream)
+        rt.cudaEventRecord(ev0[k], stream)
+        sim.step_async(it, 1)
+        launches += sim.launch_count()
+        rt.cudaEventRecord(ev1[k], stream)
+        it += 1
+    rt.cudaStreamSynchronize(stream)
+    t_wall1 = time.perf_counter()
+    dist.barrier()
+    clocks = sampler.stop()
+    sim.sync()
+    ms = []
+    for k in range(nev):
+        f = ctypes.c_float()
+        rt.cudaEventElapsedTime(ctypes.byref(f), ev0[k], ev1[k])
+        ms.append(f.value)
+    # per-kernel device time over the timed region (same stream, CUDA events)
+    names = ctypes.create_string_buffer(64 * 64)
+    kms = (ctypes.c_double * 64)()
+    kl = (ctypes.c_long * 64)()
+    capi.lib().pfag_profile_read.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_int]
+    nk = capi.lib().pfag_profile_read(sim.h, names, kms, kl, 64)
+    ktimes = {}
+    for k in range(nk):
+        nm = names.raw[64 * k:64 * (k + 1)].split(b"\0")[0].decode()
+        ktimes[nm] = (kms[k], kl[k])
+    capi.lib().pfag_set_profile(sim.h, 0)
+    stats = sim.stats()
+    step_ms_local = float(np.mean(ms))
+    total_ms_local = float(np.sum(ms))
+    total_ms = dist.max(total_ms_local)
+    value = sites * nev * ws / (total_ms * 1e-3)
+
+    # roofline of the dominant kernel
+    iters_per_step = {"cell_iters_sum": stats["cell_iters_sum"], "lum_iters": stats["lum_iters"],
+                      "ecm_iters": stats["ecm_iters"]}
+    kb = kernel_bytes(cfg, prec, iters_per_step)
+    top = max(ktimes.items(), key=lambda kv: kv[1][0]) if ktimes else ("none", (0.0, 1))
+    top_name, (top_ms, top_launches) = top
+    peak, peak_kind = measured_peak_hbm()
+    per_launch_ms = top_ms / max(top_launches, 1)
+    achieved = kb.get(top_name, 0) / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
+    total_k_ms = sum(v[0] for v in ktimes.values()) or 1.0
+    roofline = {"bound": "hbm", "kernel": top_name, "achieved": round(achieved, 1), "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": None, "share": round(top_ms / total_k_ms, 3),
+                "per_kernel_ms_per_step": {k: round(v[0] / nev, 4) for k, v in sorted(ktimes.items())},
+                "per_kernel_gbs": {k: round(kb[k] / (v[0] / max(v[1], 1) * 1e-3) / 1e9, 1)
+                                   for k, v in ktimes.items() if k in kb and v[0] > 0}}
+    sim.close()
+
+    # end to end through the public C ABI: pinned host buffers in, K steps, state out
+    e2e = run_e2e(args, cfg, p, prec, init, rt, capi, sites, dist)
+
+    result = {"value": value, "ms_per_step": dist.max(step_ms_local), "roofline": roofline, "e2e": e2e,
+              "gpu_launches": int(dist.sum(launches)), "clocks": clocks, "stats": stats,
+              "wall_ms": (t_wall1 - t_wall0) * 1e3}
+    if rank == 0 and ws == 1 and not args.no_compare:
+        result["compare"] = compare_paths(cfg, p, capi)
+    rt.cudaFree(flush)
+    return result
+
+
+def run_e2e(args, cfg, p, prec, init, rt, capi, sites, dist):
+    nsteps = args.steps
+    dtype = np.float64 if prec == 64 else np.float32
+    host = [np.ascontiguousarray(x, dtype=dtype) for x in init]
+    outs = [np.empty_like(x) for x in host]
+    rt.cudaHostRegister.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint]
+    rt.cudaHostUnregister.argtypes = [ctypes.c_void_p]
+    for a in host + outs:
+        rt.cudaHostRegister(a.ctypes.data, a.nbytes, 0)
+    sim = capi.Simulation(p, prec, capi.PATH_FUSED)
+    s_host = np.empty(cfg.ncells, np.float64)
+    dist.barrier()
+    t0 = time.perf_counter()
+    sim.upload(*host)                       # H2D of the initial state
+    for k in range(nsteps):
+        sim.step(k, 1)                      # synchronous C-ABI call, areas + centres read back
+        s_host[:] = sim.areas()[0]
+    capi.check(capi.lib().pfag_download(sim.h, *[ctypes.c_void_p(a.ctypes.data) for a in outs]))
+    t1 = time.perf_counter()
+    dist.barrier()
+    sim.close()
+    for a in host + outs:
+        rt.cudaHostUnregister(a.ctypes.data)
+    el = dist.max(t1 - t0)
+    h2d = sum(a.nbytes for a in host)
+    d2h = sum(a.nbytes for a in outs) + nsteps * cfg.ncells * (8 + 8 + 4 + 4)
+    return {"value": sites * nsteps * dist.ws / el, "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d / nsteps), "d2h_bytes_per_step": int(d2h / nsteps),
+            "steps": nsteps, "note": "pfag_upload from pinned host buffers, pfag_step per step "
+                                     "(areas and centres read back each step), pfag_download of the final state"}
+
+
+def compare_paths(cfg, p, capi, nsteps=20):
+    """fast (FP32 fused) and fused FP64 against the plain FP64 path after nsteps."""
+    res = {}
+    for key, prec, path in (("plain_f64", 64, capi.PATH_PLAIN), ("fused_f64", 64, capi.PATH_FUSED),
+                            ("fused_f32", 32, capi.PATH_FUSED)):
+        dtype = np.float64 if prec == 64 else np.float32
+        with capi.Simulation(p, prec, path) as sim:
+            sim.upload(*cfg.initial_state(dtype))
+            sim.step(0, 3)
+            t0 = time.perf_counter()
+            sim.step(3, nsteps - 3)
+            el = time.perf_counter() - t0
+            phi, rho, _, _ = sim.download()
+            res[key] = dict(phi=phi.astype(np.float64), rho=rho.astype(np.float64), s=sim.areas()[0],
+                            rate=cfg.ncells * cfg.N * cfg.N * (nsteps - 3) / el)
+    base = res["plain_f64"]
+    out = {"steps": nsteps, "plain_f64_rate": base["rate"]}
+    for key in ("fused_f64", "fused_f32"):
+        r = res[key]
+        mask = np.abs(base["phi"]) > 1e-6
+        out[key] = {"rate": r["rate"],
+                    "area_rel_max": float(np.max(np.abs(r["s"] - base["s"]) / np.abs(base["s"]))),
+                    "phi_abs_max": float(np.max(np.abs(r["phi"] - base["phi"]))),
+                    "phi_abs_max_where_phi_gt_1e-6": float(np.max(np.abs(r["phi"] - base["phi"])[mask])),
+                    "rho_rel_linf": float(np.max(np.abs(r["rho"] - base["rho"])) / np.max(np.abs(base["rho"])))}
+    return out
+
+
+def cpu_reference_rate(cfg_name: str, steps: int, warmup: int, precision: str = "fp32"):
+    """The reference's own step (oracle/_ref, g++ build, serial) on the host."""
+    from multicellular_phase_field_active_gel_organoids_b200.params import CONFIGS
+    from oracle import refrun
+    if not refrun.available(precision):
+        return None
+    code = f"""
+import sys, time, json, numpy as np
+sys.path.insert(0, {ROOT!r})
+from multicellular_phase_field_active_gel_organoids_b200.params import CONFIGS
+from oracle.refrun import RefLib
+cfg = CONFIGS[{cfg_name!r}]()
+r = RefLib({precision!r}, cfg.params())
+r.load(*cfg.initial_state(np.float64 if {precision!r} == 'fp64' else np.float32))
+for k in range({warmup}): r.step(k)
+t = time.perf_counter()
+for k in range({steps}): r.step({warmup} + k)
+el = time.perf_counter() - t
+print('RESULT', json.dumps({{'el': el}}))
+"""
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=1800)
+    line = [l for l in out.stdout.splitlines() if l.startswith("RESULT")]
+    if not line:
+        raise RuntimeError("reference run failed: " + out.stderr[-2000:])
+    el = json.loads(line[0].split(" ", 1)[1])["el"]
+    cfg = CONFIGS[cfg_name]()
+    return cfg.ncells * cfg.N * cfg.N * steps / el, el
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_info()
+    from multicellular_phase_field_active_gel_organoids_b200.params import CONFIGS
+    cfg = CONFIGS[args.config]()
+    config = {"workload": f"{args.config}: {cfg.N}x{cfg.N} periodic grid, {cfg.ncells} cells R={cfg.radius:g} "
+                          f"on a jittered hexagonal lattice, zone_size {cfg.zone_size} (FFT box {cfg.box}), "
+                          f"dx=1 dt=1e-3", "grid": cfg.N, "cells": cfg.ncells, "zone_size": cfg.zone_size,
+              "box": cfg.box, "l2": "flushed between timed steps (256 MiB write)",
+              "replicas": ws}
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        k = max(1, min(args.steps, 8))
+        w = 1 if args.warmup > 0 else 0
+        rate, el = cpu_reference_rate(args.config, k, w, "fp32")
+        sample = (f"{k} reference steps of the full {args.config} workload after {w} warm-up step, "
+                  f"shipped FP32 build (g++ -O3, OpenACC pragmas inert), one process")
+        line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": k, "warmup": w,
+                "ms_per_step": el / k * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic (seeded organoid, same generator as our arm)", "config": config,
+                "impl": "reference",
+                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
+                "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    dist = Dist(ws, rank, local, "nccl")
+    res = run_ours(args, ws, rank, local, dist)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            r = cpu_reference_rate(args.config, 2, 1, "fp32")
+            if r:
+                cpu = {"value": r[0], "unit": UNIT, "cores": 1, "kind": "reference",
+                       "sample": "2 steps (after 1 warm-up) of the full workload, reference FP32 build, 1 core"}
+        except Exception as e:  # pragma: no cover - reported, not fatal
+            cpu = {"error": str(e)[:200]}
+    dist.close()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": res["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == 32 else "f64",
+            "data": "synthetic (seeded organoid inputs generated in-process; no dataset)",
+            "config": dict(config, path="fused", precision=("f32 with f64 areas/loop sums" if args.precision == 32
+                                                            else "f64"),
+                           parallelism=f"replicas x{ws}"),
+            "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"],
+            "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
+            "active_site_updates_per_s": res["value"] * (2 * cfg.zone_size) ** 2 / cfg.N ** 2,
+            "relax_iters_last_step": res["stats"]}
+    if "compare" in res:
+        line["compare_vs_plain_f64"] = res["compare"]
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -102,8 +102,20 @@ int pfag_get_velocity(pfag_ctx *ctx, void *vx, void *vy);
  * cap stops with PFAG_E_RELAX reported at the next synchronisation. */
 int pfag_set_relax_cap(pfag_ctx *ctx, int cap);
 
+/* Per-kernel CUDA-event timing of the fused path on the context's stream.
+ * pfag_profile_read synchronises and returns the number of kernels (<= cap):
+ * names (64 bytes each), accumulated milliseconds and launch counts since the
+ * previous read. */
+int pfag_set_profile(pfag_ctx *ctx, int on);
+int pfag_profile_read(pfag_ctx *ctx, char *names, double *ms, long *launches, int cap);
+
 /* Device pointers of the state (phi, rho: [Ntot][N][N]; lum, ECM: [N][N]). */
 int pfag_device_state(pfag_ctx *ctx, void **phi, void **rho, void **lum, void **ecm);
+/* Device pointer of one named state array of the context: "phi", "phin",
+ * "rho", "rhon", "hfunc_cell", "psi", "lum", "lumn", "ECM", "ECMn",
+ * "hfunc_lum", "hfunc_ECM" (reference names, declare_tables.h:20-60);
+ * *elements receives its length.  The context keeps ownership. */
+int pfag_device_field(pfag_ctx *ctx, const char *name, void **ptr, long *elements);
 /* CUDA stream (cudaStream_t) the context enqueues on. */
 void *pfag_stream(pfag_ctx *ctx);
 /* Number of kernel launches the last pfag_step / pfag_step_async enqueued. */

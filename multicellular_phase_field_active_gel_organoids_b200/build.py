@@ -21,7 +21,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxe
 # contraction into fused multiply-adds its rounding matches a host build of the
 # reference, which keeps the far-field branch decisions (|grad phi| > 0 on the
 # 2^-54 staircase of the initial profile) identical.
-PER_FILE = {"pfag_plain.cu": ["-fmad=false"]}
+PER_FILE = {"pfag_plain.cu": ["-fmad=false"], "pfag_fused_f64.cu": ["-fmad=false"]}
 OBJ_DIR = os.path.join(HERE, "_build")
 
 

@@ -90,6 +90,9 @@ def lib() -> ctypes.CDLL:
         L.pfag_get_velocity.argtypes = [vp, vp, vp]
         L.pfag_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
                                         ctypes.POINTER(vp)]
+        L.pfag_device_field.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_long)]
+        L.pfag_set_profile.argtypes = [vp, ctypes.c_int]
+        L.pfag_profile_read.argtypes = [vp, vp, vp, vp, ctypes.c_int]
         L.pfag_stream.argtypes = [vp]
         L.pfag_stream.restype = vp
         L.pfag_launch_count.argtypes = [vp]
@@ -219,6 +222,13 @@ class Simulation:
         vy = np.empty(shape, self.dtype)
         check(lib().pfag_get_velocity(self.h, _ptr(vx), _ptr(vy)))
         return vx, vy
+
+    def device_field(self, name: str):
+        """(device pointer, element count) of a named state array."""
+        p = ctypes.c_void_p()
+        n = ctypes.c_long()
+        check(lib().pfag_device_field(self.h, name.encode(), ctypes.byref(p), ctypes.byref(n)))
+        return int(p.value or 0), int(n.value)
 
     def launch_count(self) -> int:
         return int(lib().pfag_launch_count(self.h))

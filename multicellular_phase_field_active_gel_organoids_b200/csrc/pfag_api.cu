@@ -72,6 +72,7 @@ static void free_ctx(pfag_ctx *c) {
     cudaStreamSynchronize(c->stream);
     pfag_plain_free(c);
     pfag_fused_free(c);
+    pfag_prof_free(c);
     void *bufs[] = {c->phi, c->phin, c->rho, c->rhon, c->lum, c->lumn, c->ecm, c->ecmn, c->hfunc, c->hlum,
                     c->hecm, c->psi, c->d_xc, c->d_yc, c->d_cacc, c->d_s, c->d_f0, c->d_part, c->d_scal,
                     c->d_iflags, c->d_err, c->d_vx, c->d_vy};
@@ -295,6 +296,24 @@ extern "C" int pfag_device_state(pfag_ctx *c, void **phi, void **rho, void **lum
     if (lum) *lum = c->lum;
     if (ecm) *ecm = c->ecm;
     return PFAG_OK;
+}
+
+extern "C" int pfag_device_field(pfag_ctx *c, const char *name, void **ptr, long *elements) {
+    if (!c || !name || !ptr) { pfag_set_error("null argument"); return PFAG_E_ARG; }
+    struct { const char *n; void *p; size_t cnt; } tab[] = {
+        {"phi", c->phi, c->nc}, {"phin", c->phin, c->nc}, {"rho", c->rho, c->nc}, {"rhon", c->rhon, c->nc},
+        {"hfunc_cell", c->hfunc, c->nc}, {"psi", c->psi, c->ng}, {"lum", c->lum, c->ng},
+        {"lumn", c->lumn, c->ng}, {"ECM", c->ecm, c->ng}, {"ECMn", c->ecmn, c->ng},
+        {"hfunc_lum", c->hlum, c->ng}, {"hfunc_ECM", c->hecm, c->ng}};
+    for (auto &e : tab) {
+        if (std::strcmp(e.n, name) == 0) {
+            *ptr = e.p;
+            if (elements) *elements = (long)e.cnt;
+            return PFAG_OK;
+        }
+    }
+    pfag_set_error("unknown field %s", name);
+    return PFAG_E_ARG;
 }
 
 extern "C" void *pfag_stream(pfag_ctx *c) { return c ? (void *)c->stream : nullptr; }

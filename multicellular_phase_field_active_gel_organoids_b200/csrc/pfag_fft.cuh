@@ -62,7 +62,7 @@ __device__ void fft_stages(T *base, int nseq, int sstride, int logm, const T *tw
     if (logm & 1) {
         const int half = M >> 1;
         for (int w = threadIdx.x; w < nseq * half; w += blockDim.x) {
-            const int q = w / half, b = w - q * half;
+            const int q = w >> (logm - 1), b = w & (half - 1);
             T *a = base + (size_t)q * sstride + 2 * b;
             T u = a[0], v = a[1];
             a[0] = cadd(u, v);
@@ -76,8 +76,8 @@ __device__ void fft_stages(T *base, int nseq, int sstride, int logm, const T *tw
         const int Q = 1 << s, L = Q << 2;
         const int strA = M / (2 * Q), strB = M / L;
         for (int w = threadIdx.x; w < nseq * quarter; w += blockDim.x) {
-            const int q = w / quarter, r = w - q * quarter;
-            const int grp = r / Q, k = r - grp * Q;
+            const int q = w >> (logm - 2), r = w & (quarter - 1);
+            const int grp = r >> s, k = r & (Q - 1);
             T *a = base + (size_t)q * sstride + grp * L + k;
             T x0 = a[0], x1 = a[Q], x2 = a[2 * Q], x3 = a[3 * Q];
             T wA = tw[k * strA], wB = tw[k * strB], wB2 = tw[(k + Q) * strB];
@@ -99,7 +99,7 @@ template <typename T>
 __device__ void bitrev_permute(T *base, int nseq, int sstride, int logm) {
     const int M = 1 << logm;
     for (int w = threadIdx.x; w < nseq * M; w += blockDim.x) {
-        const int q = w / M, i = w - q * M;
+        const int q = w >> logm, i = w & (M - 1);
         const int r = bitrev(i, logm);
         if (i < r) {
             T *a = base + (size_t)q * sstride;

@@ -1,1172 +1,19 @@
-// Fused path: the same step as the plain path (and the reference loop body,
-// main_code/run_with_active_gels.cpp:123-182), restricted to the sites that
-// can change and fused into 13 launches per step with no host round trip.
-//
-// Exactness of the restriction.  Every per-cell write of the reference step
-// lands in that cell's zone [xc-z, xc+z)^2, and hfunc_cell starts at zero, so
-// outside the bounding rectangle B_n of all zones the cell has visited,
-// hfunc_cell[n] is exactly 0 and phi[n] keeps its initial value.  Upload
-// checks that the initial phi[n] is <= 0.5 outside the first zone; then the
-// full-grid sums of the reference (centroid counts useful_functions.cpp:
-// 208-219, areas :179-184, psi :315-318) equal sums over B_n, and psi skips
-// only +0.0 terms (bit-identical).  Full-grid work arrays the reference fills
-// (norm_grad_phi, J_x/J_y, prod_norm_delta, temp_phase, the parameter maps,
-// pi_*) are recomputed on the fly where they are read.
-//
-// Spectral solve (rho_functions.cpp:409-471) per cell on the M x M box with
-// hand-written shared-memory FFTs in five passes:
-//   A rows:    stress pi_xx + i pi_yy and pi_xy, row FFT; reaction R stored
-//   B columns: column FFT, unpack, velocity (rho_functions.cpp:133-190),
-//              Hermitian projection packing Re(v_x) + i Re(v_y), column IFFT
-//   C rows:    row IFFT -> v; rho v / M^2 packed; row FFT
-//   D columns: column FFT, unpack, divergence term of update_fft_rho
-//              (rho_functions.cpp:230-249), Hermitian projection, column IFFT
-//   E rows:    row IFFT; rho_new = rho + dt R + Re(.)/M^2
-// By linearity of the transform this equals Re(IFFT(FFT(rho) + dt FFT(R) + D))/M^2
-// of the reference, without the two round-trip transforms of rho and R.
-#include "pfag_internal.cuh"
-#include "pfag_fft.cuh"
-#include <cooperative_groups.h>
-#include <algorithm>
-#include <cmath>
-#include <vector>
+// Fused path: precision dispatch and resource release (kernels in pfag_fused_impl.cuh,
+// instantiated in pfag_fused_f64.cu and pfag_fused_f32.cu).
+#include "pfag_fused_impl.cuh"
+#include <cstring>
 
-namespace cg = cooperative_groups;
-
-namespace {
-
-constexpr int FT = 256;           // threads per block of the fused kernels
-constexpr int SBLK = 32;          // blocks per cell of the support-rectangle reductions
-constexpr int RT_I = 16, RT_J = 32;  // reshaping tile (rows x cols)
-
-struct FusedRes {
-    void *Y1, *Y2;          // complex [Ntot][M][M]
-    void *Rb;               // real [Ntot][M][M]   reaction -deg*rho + gen*P on the box
-    unsigned char *clsT;    // [Ntot][M(j)][M(i)]  apical/basal/lateral class, transposed
-    void *Jc;               // real [Ntot][2][W][W] normals on zone + 1 ring, W = 2z+2
-    void *Jl;               // real [4][N][N] lumen / ECM normals
-    int4 *rect;             // [Ntot] support rectangle (i0, i1, j0, j1), half-open
-    double *part_s;         // [Ntot][SBLK]
-    double *part_r;         // [Ntot][tpc]
-    double *part_e;         // [npsi] sum_ecm partials
-    double *part_l;         // [2][coop_l]
-    int *cK, *cdone, *ccnt; // per cell
-    int *lK, *ldone, *lcnt; // [2] lumen, ECM
-    int tpc, tiles_i, tiles_j;
-    int npsi;
-    int coop_r, coop_l;     // co-resident block counts of the persistent kernels
-    int logm, rows_blk, grp_cols;
-    size_t smemA, smemB, smemC, smemD, smemE;
-    cudaGraph_t graph;
-    cudaGraphExec_t gexec;
-    bool graph_ok;
-    int graph_it;           // steps in the captured graph (1)
-};
-
-template <typename real>
-__device__ __forceinline__ int map_class_f(real ph, real l, real e, real pm, real pp) {
-    // create_turnover_rates_tensions, rho_functions.cpp:324-353
-    real c1l = ph * l, c1e = ph * e;
-    int index;
-    real mx;
-    if (c1l > c1e) { index = 0; mx = c1l; } else { index = 1; mx = c1e; }
-    real c1c2 = ph * pm;
-    if (c1c2 > mx) { index = 2; mx = c1c2; }
-    real c1c3 = ph * pp;
-    if (c1c3 > mx) { index = 3; }
-    return index == 3 ? 2 : index;
-}
-
-__device__ __forceinline__ double block_sum_d(double v) {
-    __shared__ double sh[32];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    __syncthreads();
-    if (l == 0) sh[w] = v;
-    __syncthreads();
-    double r = 0.0;
-    if (threadIdx.x == 0)
-        for (int k = 0; k < (int)(blockDim.x >> 5); k++) r += sh[k];
-    __syncthreads();
-    return r;
-}
-
-// ---- support-rectangle centroid (find_centres_cells, useful_functions.cpp:193-227)
-template <typename real>
-__global__ void kf_centroid(const real *__restrict__ phi, const int4 *__restrict__ rect, int N,
-                            long long *__restrict__ acc) {
-    const int n = blockIdx.y;
-    const int4 r = rect[n];
-    const int w = r.w - r.z;
-    const long long tot = (long long)(r.y - r.x) * w;
-    long long cnt = 0, sx = 0, sy = 0;
-    const real *p = phi + (size_t)n * N * N;
-    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += (long long)gridDim.x * blockDim.x) {
-        const int i = r.x + (int)(k / w), j = r.z + (int)(k % w);
-        if (p[(size_t)i * N + j] > (real)0.5) { cnt++; sx += i; sy += j; }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        cnt += __shfl_down_sync(0xffffffffu, cnt, o);
-        sx += __shfl_down_sync(0xffffffffu, sx, o);
-        sy += __shfl_down_sync(0xffffffffu, sy, o);
-    }
-    if ((threadIdx.x & 31) == 0 && cnt) {
-        atomicAdd((unsigned long long *)&acc[3 * n + 0], (unsigned long long)cnt);
-        atomicAdd((unsigned long long *)&acc[3 * n + 1], (unsigned long long)sx);
-        atomicAdd((unsigned long long *)&acc[3 * n + 2], (unsigned long long)sy);
-    }
-}
-
-// centroid, zone check (clamped so no kernel can leave the grid), B_n union zone
-__global__ void kf_centroid_finalize(const long long *__restrict__ acc, int Ntot, int N, int zone,
-                                     int *__restrict__ xc, int *__restrict__ yc, int4 *__restrict__ rect,
-                                     unsigned *__restrict__ err) {
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= Ntot) return;
-    long long c = acc[3 * n];
-    int x, y;
-    if (c == 0) {
-        atomicOr(err, ERRBIT_EMPTY_CELL);
-        x = N / 2; y = N / 2;
-    } else {
-        x = (int)(acc[3 * n + 1] / c);
-        y = (int)(acc[3 * n + 2] / c);
-    }
-    if (x - zone < 1 || x + zone > N - 1 || y - zone < 1 || y + zone > N - 1) {
-        atomicOr(err, ERRBIT_ZONE);
-        x = min(max(x, zone + 1), N - 1 - zone);
-        y = min(max(y, zone + 1), N - 1 - zone);
-    }
-    xc[n] = x;
-    yc[n] = y;
-    int4 r = rect[n];
-    r.x = min(r.x, x - zone); r.y = max(r.y, x + zone);
-    r.z = min(r.z, y - zone); r.w = max(r.w, y + zone);
-    rect[n] = r;
-}
-
-// ---- hfunc on the zone (useful_functions.cpp:233-251) + areas over B_n (:168-190)
-template <typename real>
-__global__ void kf_hfunc_area(const real *__restrict__ phi, real *__restrict__ hfunc, const int *__restrict__ xc,
-                              const int *__restrict__ yc, const int4 *__restrict__ rect, int N, int z, double dx2,
-                              double *__restrict__ part) {
-    const int n = blockIdx.y;
-    const int4 r = rect[n];
-    const int w = r.w - r.z;
-    const long long tot = (long long)(r.y - r.x) * w;
-    const int zi0 = xc[n] - z, zj0 = yc[n] - z;
-    const size_t base = (size_t)n * N * N;
-    double acc = 0.0;
-    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += (long long)gridDim.x * blockDim.x) {
-        const int i = r.x + (int)(k / w), j = r.z + (int)(k % w);
-        const size_t o = base + (size_t)i * N + j;
-        real h;
-        if (i >= zi0 && i < zi0 + 2 * z && j >= zj0 && j < zj0 + 2 * z) {
-            const real f = phi[o];
-            h = f * f * ((real)3.0 - (real)2.0 * f);
-            hfunc[o] = h;
-        } else {
-            h = hfunc[o];
-        }
-        acc += (double)h * dx2;
-    }
-    double s = block_sum_d(acc);
-    if (threadIdx.x == 0) part[(size_t)n * gridDim.x + blockIdx.x] = s;
-}
-
-__global__ void kf_area_finalize(const double *__restrict__ part, int nblk, int Ntot, double alpha, double s0,
-                                 double *__restrict__ s, double *__restrict__ f0) {
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= Ntot) return;
-    double a = 0.0;
-    for (int b = 0; b < nblk; b++) a += part[(size_t)n * nblk + b];
-    s[n] = a;
-    f0[n] = alpha * (s0 - a);
-}
-
-// ---- psi = sum_n hfunc_cell[n] over the cells whose B_n covers the tile,
-//      h(lum), h(ECM) and the sum_ecm partials (useful_functions.cpp:272-322,
-//      cell_phase_functions.cpp:376-386)
-template <typename real>
-__global__ void kf_psi(const real *__restrict__ hfunc, const int4 *__restrict__ rect, int Ntot, int N,
-                       const real *__restrict__ lum, const real *__restrict__ ecm, real *__restrict__ psi,
-                       real *__restrict__ hl, real *__restrict__ he, double dx2, double *__restrict__ part) {
-    __shared__ int list[1024];
-    __shared__ int nlist;
-    const int ti0 = blockIdx.y * 32, tj0 = blockIdx.x * 32;
-    if (threadIdx.x == 0) nlist = 0;
-    __syncthreads();
-    for (int n = threadIdx.x; n < Ntot; n += blockDim.x) {
-        int4 r = rect[n];
-        if (r.x < ti0 + 32 && r.y > ti0 && r.z < tj0 + 32 && r.w > tj0) {
-            int slot = atomicAdd(&nlist, 1);
-            if (slot < 1024) list[slot] = n;
-        }
-    }
-    __syncthreads();
-    const int nl = min(nlist, 1024);
-    // ascending cell order (the reference sums n = 0 .. Ntot-1)
-    if (threadIdx.x == 0) {
-        for (int a = 1; a < nl; a++) {
-            int v = list[a], b = a - 1;
-            while (b >= 0 && list[b] > v) { list[b + 1] = list[b]; b--; }
-            list[b + 1] = v;
-        }
-    }
-    __syncthreads();
-    double acc = 0.0;
-    for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
-        const int i = ti0 + (e >> 5), j = tj0 + (e & 31);
-        if (i >= N || j >= N) continue;
-        const size_t s = (size_t)i * N + j;
-        real sum = (real)0.0;
-        for (int q = 0; q < nl; q++) {
-            const int n = list[q];
-            const int4 r = rect[n];
-            if (i >= r.x && i < r.y && j >= r.z && j < r.w) sum += hfunc[(size_t)n * N * N + s];
-        }
-        psi[s] = sum;
-        const real a = lum[s], b = ecm[s];
-        hl[s] = a * a * ((real)3.0 - (real)2.0 * a);
-        const real hb = b * b * ((real)3.0 - (real)2.0 * b);
-        he[s] = hb;
-        acc += (double)hb * dx2;
-    }
-    double t = block_sum_d(acc);
-    if (threadIdx.x == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = t;
-}
-
-// ---- box passes -------------------------------------------------------------
-struct BoxArgs {
-    int N, z, M, logm, Ntot;
-    double c4, sigma, dt, kfac, friction, dx;
-    double deg[3], gen[3], a_ort[3], a_tan[3], visc[3], bb[3];
-};
-
-__device__ __forceinline__ int wrapk(int i, int M) { return i < M / 2 ? i : i - M; }
-
-// Pass A: rows [i0, i0+R) of cell n's box
-template <typename real>
-__global__ void kf_boxA(const real *__restrict__ phi, const real *__restrict__ rho, const real *__restrict__ lum,
-                        const real *__restrict__ ecm, const int *__restrict__ xc, const int *__restrict__ yc,
-                        BoxArgs a, int R, typename Cplx<real>::type *__restrict__ Y1,
-                        typename Cplx<real>::type *__restrict__ Y2, real *__restrict__ Rb,
-                        unsigned char *__restrict__ clsT) {
-    typedef typename Cplx<real>::type cx;
-    extern __shared__ unsigned char smraw[];
-    cx *tw = (cx *)smraw;
-    const int M = a.M, N = a.N;
-    cx *zz = tw + M;            // [2R][M]: rows of z1 then rows of z2
-    fft_twiddles(tw, M);
-    const int n = blockIdx.y, i0 = blockIdx.x * R;
-    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
-    const int n1 = (n == 0) ? a.Ntot - 1 : n - 1;
-    const int n2 = (n == a.Ntot - 1) ? 0 : n + 1;
-    const size_t NN = (size_t)N * N;
-    const real *p = phi + (size_t)n * NN;
-    const real c4 = (real)a.c4, sigma = (real)a.sigma;
-    for (int e = threadIdx.x; e < R * M; e += blockDim.x) {
-        const int r = e / M, j = e - r * M;
-        const int i = i0 + r;
-        const int gi = bi + i, gj = bj + j;
-        const size_t s = (size_t)gi * N + gj;
-        const real f = p[s];
-        const real dxp = p[s + N] - p[s - N];
-        const real dyp = p[s + 1] - p[s - 1];
-        const real g = sqrt(c4 * (dxp * dxp + dyp * dyp));
-        const int cls = map_class_f<real>(f, lum[s], ecm[s], phi[(size_t)n1 * NN + s], phi[(size_t)n2 * NN + s]);
-        const real rr = rho[(size_t)n * NN + s];
-        const real at = (real)a.a_tan[cls], ao = (real)a.a_ort[cls], b = (real)a.bb[cls];
-        // compute_pi_xx/yy/xy, rho_functions.cpp:47-51, :75-79, :105-109
-        real xx = -at * rr * rr * rr + b * rr * rr * rr * rr;
-        real yy = xx, xy = (real)0.0;
-        if (g > (real)0.0) {
-            xx += (at - ao) * rr * rr * rr * c4 * dxp * dxp / g / g;
-            yy += (at - ao) * rr * rr * rr * c4 * dyp * dyp / g / g;
-            xy += (at - ao) * rr * rr * rr * c4 * dxp * dyp / g / g;
-        }
-        // create_deg_gen with compute_prod_norm_delta, rho_functions.cpp:25, :205
-        const real P = g * exp(-(f - (real)0.5) * (f - (real)0.5) / (real)2.0 / sigma / sigma) /
-                       sqrt((real)(2.0 * M_PI)) / sigma;
-        Rb[((size_t)n * M + i) * M + j] = -(real)a.deg[cls] * rr + (real)a.gen[cls] * P;
-        clsT[((size_t)n * M + j) * M + i] = (unsigned char)cls;
-        const int br = bitrev(j, a.logm);
-        cx v1, v2;
-        v1.x = xx; v1.y = yy;
-        v2.x = xy; v2.y = (real)0.0;
-        zz[(size_t)r * M + br] = v1;
-        zz[(size_t)(R + r) * M + br] = v2;
-    }
-    __syncthreads();
-    fft_stages(zz, 2 * R, M, a.logm, tw, false);
-    for (int e = threadIdx.x; e < R * M; e += blockDim.x) {
-        const int r = e / M, k = e - r * M;
-        const size_t o = ((size_t)n * M + i0 + r) * M + k;
-        Y1[o] = zz[(size_t)r * M + k];
-        Y2[o] = zz[(size_t)(R + r) * M + k];
-    }
-}
-
-// update_rho_velocity (rho_functions.cpp:153-186) at one wavevector
-template <typename real, typename cx>
-__device__ __forceinline__ void velocity_at(real kx, real ky, real et, real friction, cx pxx, cx pyy, cx pxy,
-                                            cx &vx, cx &vy) {
-    const real A = friction + (real)2.0 * et * (kx * kx + ky * ky / (real)2.0);
-    const real D = -((real)4.0 * et * et * kx * kx * ky * ky + friction * friction +
-                     (real)3.0 * et * friction * (kx * kx + ky * ky) +
-                     (real)2.0 * et * et * (kx * kx * kx * kx + ky * ky * ky * ky));
-    vy.x = (real)0.0 + et * kx * ky * (kx * pxx.y + ky * pxy.y);
-    vy.x -= A * (ky * pyy.y + kx * pxy.y);
-    vy.x /= D;
-    vy.y = (real)0.0 - et * kx * ky * (kx * pxx.x + ky * pxy.x);
-    vy.y += A * (ky * pyy.x + kx * pxy.x);
-    vy.y /= D;
-    vx.x = (real)0.0 + (kx * pxx.y + ky * pxy.y - et * kx * ky * vy.x);
-    vx.x /= A;
-    vx.y = (real)0.0 + (-kx * pxx.x - ky * pxy.x - et * kx * ky * vy.y);
-    vx.y /= A;
-}
-
-// Column slots of a pass B/D block: primaries c0..c0+np-1 (c <= M/2), then the
-// partners M - c of the primaries that are not their own partner.
-struct ColSlots {
-    int np, ns;
-    int col[64];
-    int partner[32];
-};
-
-__device__ __forceinline__ void make_slots(ColSlots &cs, int c0, int G, int M) {
-    cs.np = min(G, M / 2 + 1 - c0);
-    cs.ns = cs.np;
-    for (int s = 0; s < cs.np; s++) {
-        const int c = c0 + s;
-        cs.col[s] = c;
-        const int pc = (M - c) % M;
-        if (pc == c) cs.partner[s] = s;
-        else { cs.col[cs.ns] = pc; cs.partner[s] = cs.ns; cs.ns++; }
-    }
-}
-
-template <typename cx>
-__device__ void load_cols(cx *dst, int sstride, const cx *__restrict__ src, const ColSlots &cs, int M, int logm) {
-    for (int e = threadIdx.x; e < cs.ns * M; e += blockDim.x) {
-        const int i = e / cs.ns, sl = e - i * cs.ns;
-        dst[(size_t)sl * sstride + bitrev(i, logm)] = src[(size_t)i * M + cs.col[sl]];
-    }
-}
-
-template <typename cx>
-__device__ void store_cols(cx *__restrict__ dstg, const cx *src, int sstride, const ColSlots &cs, int M) {
-    for (int e = threadIdx.x; e < cs.ns * M; e += blockDim.x) {
-        const int i = e / cs.ns, sl = e - i * cs.ns;
-        dstg[(size_t)i * M + cs.col[sl]] = src[(size_t)sl * sstride + i];
-    }
-}
-
-// Enumerate the disjoint pairs {k, -k} of the slots; calls f(slot_a, kx_a, slot_b, kx_b).
-template <typename F>
-__device__ __forceinline__ void for_pairs(const ColSlots &cs, int M, F f) {
-    const int half = M / 2;
-    int total = 0;
-    for (int s = 0; s < cs.np; s++) total += (cs.partner[s] == s) ? (half + 1) : M;
-    for (int w = threadIdx.x; w < total; w += blockDim.x) {
-        int rem = w, s = 0;
-        for (; s < cs.np; s++) {
-            const int cnt = (cs.partner[s] == s) ? (half + 1) : M;
-            if (rem < cnt) break;
-            rem -= cnt;
-        }
-        const int kx = rem, kx2 = (M - kx) % M;
-        f(s, kx, cs.partner[s], kx2);
-    }
-}
-
-template <typename real>
-__global__ void kf_boxB(typename Cplx<real>::type *__restrict__ Y1, const typename Cplx<real>::type *__restrict__ Y2,
-                        const unsigned char *__restrict__ clsT, BoxArgs a, int G) {
-    typedef typename Cplx<real>::type cx;
-    extern __shared__ unsigned char smraw[];
-    const int M = a.M, S = M + 1;
-    cx *tw = (cx *)smraw;
-    fft_twiddles(tw, M);
-    __shared__ ColSlots cs;
-    const int n = blockIdx.y;
-    if (threadIdx.x == 0) make_slots(cs, blockIdx.x * G, G, M);
-    __syncthreads();
-    cx *Z1 = tw + M, *Z2 = Z1 + (size_t)cs.ns * S;
-    const cx *y1 = Y1 + (size_t)n * M * M, *y2 = Y2 + (size_t)n * M * M;
-    load_cols(Z1, S, y1, cs, M, a.logm);
-    load_cols(Z2, S, y2, cs, M, a.logm);
-    __syncthreads();
-    // both fields in one call: Z2 follows Z1 with the same stride
-    fft_stages(Z1, 2 * cs.ns, S, a.logm, tw, false);
-    const unsigned char *cl = clsT + (size_t)n * M * M;
-    const real kf = (real)0.0;
-    (void)kf;
-    for_pairs(cs, M, [&](int sa, int ka, int sb, int kb) {
-        const cx z1a = Z1[(size_t)sa * S + ka], z1b = Z1[(size_t)sb * S + kb];
-        const cx z2a = Z2[(size_t)sa * S + ka], z2b = Z2[(size_t)sb * S + kb];
-        // unpack the two real fields packed as pi_xx + i pi_yy
-        cx pxx_a, pyy_a, pxx_b, pyy_b;
-        pxx_a.x = (real)0.5 * (z1a.x + z1b.x); pxx_a.y = (real)0.5 * (z1a.y - z1b.y);
-        pyy_a.x = (real)0.5 * (z1a.y + z1b.y); pyy_a.y = (real)0.5 * (z1b.x - z1a.x);
-        pxx_b.x = pxx_a.x; pxx_b.y = -pxx_a.y;
-        pyy_b.x = pyy_a.x; pyy_b.y = -pyy_a.y;
-        const int ca = cs.col[sa], cb = cs.col[sb];
-        const real kxa = (real)(a.kfac * wrapk(ka, M)), kya = (real)(a.kfac * wrapk(ca, M));
-        const real kxb = (real)(a.kfac * wrapk(kb, M)), kyb = (real)(a.kfac * wrapk(cb, M));
-        const real eta_a = (real)a.visc[cl[(size_t)ca * M + ka]];
-        const real eta_b = (real)a.visc[cl[(size_t)cb * M + kb]];
-        const real fr = (real)a.friction;
-        cx vxa, vya, vxb, vyb;
-        velocity_at<real, cx>(kxa, kya, eta_a, fr, pxx_a, pyy_a, z2a, vxa, vya);
-        velocity_at<real, cx>(kxb, kyb, eta_b, fr, pxx_b, pyy_b, z2b, vxb, vyb);
-        // Hermitian parts: H(X)(k) = (X(k) + conj(X(-k)))/2, packed H(vx) + i H(vy)
-        cx hx, hy;
-        hx.x = (real)0.5 * (vxa.x + vxb.x); hx.y = (real)0.5 * (vxa.y - vxb.y);
-        hy.x = (real)0.5 * (vya.x + vyb.x); hy.y = (real)0.5 * (vya.y - vyb.y);
-        cx pa, pb;
-        pa.x = hx.x - hy.y; pa.y = hx.y + hy.x;
-        pb.x = hx.x + hy.y; pb.y = hy.x - hx.y;
-        Z1[(size_t)sa * S + ka] = pa;
-        if (!(sa == sb && ka == kb)) Z1[(size_t)sb * S + kb] = pb;
-    });
-    __syncthreads();
-    bitrev_permute(Z1, cs.ns, S, a.logm);
-    fft_stages(Z1, cs.ns, S, a.logm, tw, true);
-    store_cols(Y1 + (size_t)n * M * M, Z1, S, cs, M);
-}
-
-template <typename real>
-__global__ void kf_boxC(const typename Cplx<real>::type *__restrict__ Y1, typename Cplx<real>::type *__restrict__ Y2,
-                        const real *__restrict__ rho, const int *__restrict__ xc, const int *__restrict__ yc,
-                        BoxArgs a, int R, real *__restrict__ vdx, real *__restrict__ vdy) {
-    typedef typename Cplx<real>::type cx;
-    extern __shared__ unsigned char smraw[];
-    const int M = a.M, N = a.N;
-    cx *tw = (cx *)smraw;
-    cx *zz = tw + M;
-    fft_twiddles(tw, M);
-    const int n = blockIdx.y, i0 = blockIdx.x * R;
-    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
-    for (int e = threadIdx.x; e < R * M; e += blockDim.x) {
-        const int r = e / M, j = e - r * M;
-        zz[(size_t)r * M + bitrev(j, a.logm)] = Y1[((size_t)n * M + i0 + r) * M + j];
-    }
-    __syncthreads();
-    fft_stages(zz, R, M, a.logm, tw, true);
-    const real mm = (real)((double)M * (double)M);
-    const real *rh = rho + (size_t)n * N * N;
-    // each thread owns the same set of e in both loops, so the permuted store
-    // below may only be issued after every thread has read its values
-    cx vals[8];
-    int cntv = 0;
-    for (int e = threadIdx.x; e < R * M; e += blockDim.x) {
-        const int r = e / M, j = e - r * M;
-        const cx v = zz[(size_t)r * M + j];
-        const real rr = rh[(size_t)(bi + i0 + r) * N + bj + j];
-        // load_fft_rho_v, rho_functions.cpp:279: rho * Re(IFFT(v)) / M^2
-        cx q;
-        q.x = rr * v.x / mm;
-        q.y = rr * v.y / mm;
-        if (vdx) {
-            const size_t o = ((size_t)n * M + i0 + r) * M + j;
-            vdx[o] = v.x / mm;
-            vdy[o] = v.y / mm;
-        }
-        vals[cntv++] = q;
-    }
-    __syncthreads();
-    cntv = 0;
-    for (int e = threadIdx.x; e < R * M; e += blockDim.x) {
-        const int r = e / M, j = e - r * M;
-        zz[(size_t)r * M + bitrev(j, a.logm)] = vals[cntv++];
-    }
-    __syncthreads();
-    fft_stages(zz, R, M, a.logm, tw, false);
-    for (int e = threadIdx.x; e < R * M; e += blockDim.x) {
-        const int r = e / M, k = e - r * M;
-        Y2[((size_t)n * M + i0 + r) * M + k] = zz[(size_t)r * M + k];
-    }
-}
-
-template <typename real>
-__global__ void kf_boxD(typename Cplx<real>::type *__restrict__ Y1, const typename Cplx<real>::type *__restrict__ Y2,
-                        BoxArgs a, int G) {
-    typedef typename Cplx<real>::type cx;
-    extern __shared__ unsigned char smraw[];
-    const int M = a.M, S = M + 1;
-    cx *tw = (cx *)smraw;
-    fft_twiddles(tw, M);
-    __shared__ ColSlots cs;
-    const int n = blockIdx.y;
-    if (threadIdx.x == 0) make_slots(cs, blockIdx.x * G, G, M);
-    __syncthreads();
-    cx *W = tw + M;
-    load_cols(W, S, Y2 + (size_t)n * M * M, cs, M, a.logm);
-    __syncthreads();
-    fft_stages(W, cs.ns, S, a.logm, tw, false);
-    const real dtk = (real)(a.dt * a.kfac);
-    for_pairs(cs, M, [&](int sa, int ka, int sb, int kb) {
-        const cx wa = W[(size_t)sa * S + ka], wb = W[(size_t)sb * S + kb];
-        // (rho vx)^ = (W(k) + conj W(-k))/2, (rho vy)^ = (W(k) - conj W(-k))/(2i)
-        cx A1, B1, A2, B2;
-        A1.x = (real)0.5 * (wa.x + wb.x); A1.y = (real)0.5 * (wa.y - wb.y);
-        B1.x = (real)0.5 * (wa.y + wb.y); B1.y = (real)0.5 * (wb.x - wa.x);
-        A2.x = A1.x; A2.y = -A1.y;
-        B2.x = B1.x; B2.y = -B1.y;
-        const real ir1 = (real)wrapk(ka, M), jr1 = (real)wrapk(cs.col[sa], M);
-        const real ir2 = (real)wrapk(kb, M), jr2 = (real)wrapk(cs.col[sb], M);
-        // update_fft_rho, rho_functions.cpp:243-247: delta = -i dt k (ir A + jr B)
-        cx F1, F2, D1, D2;
-        F1.x = ir1 * A1.x + jr1 * B1.x; F1.y = ir1 * A1.y + jr1 * B1.y;
-        F2.x = ir2 * A2.x + jr2 * B2.x; F2.y = ir2 * A2.y + jr2 * B2.y;
-        D1.x = dtk * F1.y; D1.y = -dtk * F1.x;
-        D2.x = dtk * F2.y; D2.y = -dtk * F2.x;
-        cx ha, hb;
-        ha.x = (real)0.5 * (D1.x + D2.x); ha.y = (real)0.5 * (D1.y - D2.y);
-        hb.x = ha.x; hb.y = -ha.y;
-        W[(size_t)sa * S + ka] = ha;
-        if (!(sa == sb && ka == kb)) W[(size_t)sb * S + kb] = hb;
-    });
-    __syncthreads();
-    bitrev_permute(W, cs.ns, S, a.logm);
-    fft_stages(W, cs.ns, S, a.logm, tw, true);
-    store_cols(Y1 + (size_t)n * M * M, W, S, cs, M);
-}
-
-template <typename real>
-__global__ void kf_boxE(const typename Cplx<real>::type *__restrict__ Y1, const real *__restrict__ rho,
-                        const real *__restrict__ Rb, real *__restrict__ rhon, const int *__restrict__ xc,
-                        const int *__restrict__ yc, BoxArgs a, int R) {
-    typedef typename Cplx<real>::type cx;
-    extern __shared__ unsigned char smraw[];
-    const int M = a.M, N = a.N;
-    cx *tw = (cx *)smraw;
-    cx *zz = tw + M;
-    fft_twiddles(tw, M);
-    const int n = blockIdx.y, i0 = blockIdx.x * R;
-    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
-    for (int e = threadIdx.x; e < R * M; e += blockDim.x) {
-        const int r = e / M, j = e - r * M;
-        zz[(size_t)r * M + bitrev(j, a.logm)] = Y1[((size_t)n * M + i0 + r) * M + j];
-    }
-    __syncthreads();
-    fft_stages(zz, R, M, a.logm, tw, true);
-    const real mm = (real)((double)M * (double)M), dt = (real)a.dt;
-    const size_t NN = (size_t)N * N;
-    for (int e = threadIdx.x; e < R * M; e += blockDim.x) {
-        const int r = e / M, j = e - r * M;
-        const size_t s = (size_t)n * NN + (size_t)(bi + i0 + r) * N + bj + j;
-        const real rr = rho[s];
-        rhon[s] = rr + dt * Rb[((size_t)n * M + i0 + r) * M + j] + zz[(size_t)r * M + j].x / mm;
-    }
-}
-
-// ---- phi update (cell_phase_functions.cpp:126-217) + normals
-//      (useful_functions.cpp:356-388 with the periodic ghost map of :391-420)
-template <typename real>
-__global__ void kf_update(const real *__restrict__ phi, real *__restrict__ phin, const real *__restrict__ rho,
-                          const real *__restrict__ hfunc, const double *__restrict__ f0,
-                          const real *__restrict__ psi, const real *__restrict__ hl, const real *__restrict__ he,
-                          const int *__restrict__ xc, const int *__restrict__ yc, DevParams P,
-                          real *__restrict__ Jc) {
-    const int n = blockIdx.z, N = P.N, z = P.zone, W = 2 * z + 2;
-    const int ii = blockIdx.y * blockDim.y + threadIdx.y, jj = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ii >= W || jj >= W) return;
-    const int gi = xc[n] - z - 1 + ii, gj = yc[n] - z - 1 + jj;
-    const size_t NN = (size_t)N * N, base = (size_t)n * NN;
-    const real *p = phi + base;
-    const real dx = (real)P.dx;
-    const real c4 = (real)(1.0 / P.dx / P.dx / 4.0), inv2dx = (real)(1.0 / (2.0 * P.dx));
-    {
-        const int si = ghost_src(gi, N), sj = ghost_src(gj, N);
-        const size_t c = (size_t)si * N + sj;
-        const real a = p[c + N] - p[c - N], b = p[c + 1] - p[c - 1];
-        const real g = sqrt(c4 * (a * a + b * b));
-        real *J = Jc + (size_t)n * 2 * W * W;
-        J[(size_t)ii * W + jj] = (g > (real)0.0) ? inv2dx * a / g : (real)0.0;
-        J[(size_t)W * W + (size_t)ii * W + jj] = (g > (real)0.0) ? inv2dx * b / g : (real)0.0;
-    }
-    const size_t c = (size_t)gi * N + gj, o = base + c;
-    const bool in_zone = ii >= 1 && ii <= 2 * z && jj >= 1 && jj <= 2 * z;
-    if (!in_zone) { phin[o] = p[c]; return; }
-    const real dt = (real)P.dt, tau = (real)P.tau, sigma = (real)P.sigma;
-    const real f = p[c];
-    const real a = p[c + N] - p[c - N], b = p[c + 1] - p[c - 1];
-    const real gg = sqrt(c4 * (a * a + b * b));
-    real pn = f;
-    if (gg > (real)0.0) {
-        const real *r = rho + base;
-        pn -= (real)P.cpl / tau * (dt / dx / dx / (real)4.0) *
-              exp(-(f - (real)0.5) * (f - (real)0.5) / (real)2.0 / sigma / sigma) / sqrt((real)(2.0 * M_PI)) / sigma *
-              ((r[c + N] - r[c - N]) * a + (r[c + 1] - r[c - 1]) * b) / gg;
-    }
-    const real *hh = hfunc + base;
-    auto T = [&](size_t k) { return psi[k] - hh[k]; };
-    const real Tc = T(c);
-    const real LT = lap9<real>(Tc, T(c + N), T(c - N), T(c + 1), T(c - 1), T(c + N + 1), T(c + N - 1),
-                               T(c - N - 1), T(c - N + 1));
-    const real Ll = lap9<real>(hl[c], hl[c + N], hl[c - N], hl[c + 1], hl[c - 1], hl[c + N + 1], hl[c + N - 1],
-                               hl[c - N - 1], hl[c - N + 1]);
-    const real Le = lap9<real>(he[c], he[c + N], he[c - N], he[c + 1], he[c - 1], he[c + N + 1], he[c + N - 1],
-                               he[c - N - 1], he[c - N + 1]);
-    const real q4 = (real)4.0 * dx * dx;
-    pn += ((real)1.0 / tau) * f * ((real)1.0 - f) * dt *
-          ((real)f0[n] - (real)P.beta * Tc + (real)P.eta * LT / q4 - (real)P.beta_lum_cells * hl[c] +
-           (real)P.eta_lum_cells * Ll / q4 - (real)P.beta_ECM_cells * he[c] + (real)P.eta_ECM_cells * Le / q4);
-    phin[o] = pn;
-}
-
-// ---- persistent reshaping of all cells (cell_phase_functions.cpp:461-579)
-struct ReshArgs {
-    int N, z, Ntot, tpc, tiles_i, tiles_j, cap, rimax;
-    double A, B, scale, thr;
-    int *K, *done, *cnt;
-    double *part;
-    unsigned *err;
-};
-
-template <typename real>
-__global__ void kf_reshape(real *__restrict__ phi, real *__restrict__ phin, const real *__restrict__ Jc,
-                           const int *__restrict__ xc, const int *__restrict__ yc, ReshArgs a) {
-    cg::grid_group grid = cg::this_grid();
-    const int N = a.N, z = a.z, W = 2 * z + 2;
-    const real A = (real)a.A, B = (real)a.B;
-    const size_t NN = (size_t)N * N;
-    const int total = a.Ntot * a.tpc;
-    __shared__ int s_last, s_skip;
-    for (int it = 1; it <= a.cap; it++) {
-        real *P = (it & 1) ? phin : phi;
-        real *Q = (it & 1) ? phi : phin;
-        for (int t = blockIdx.x; t < total; t += gridDim.x) {
-            const int n = t / a.tpc, tile = t - n * a.tpc;
-            // a cell converged at iteration d is skipped from iteration d+1 on
-            if (threadIdx.x == 0) {
-                const int d = *(volatile int *)&a.done[n];
-                s_skip = (d != 0 && d < it);
-            }
-            __syncthreads();
-            const bool skip = s_skip;
-            __syncthreads();
-            if (skip) continue;
-            const int ti = tile / a.tiles_j, tj = tile - ti * a.tiles_j;
-            const int zi0 = xc[n] - z, zj0 = yc[n] - z;
-            const real *Jx = Jc + (size_t)n * 2 * W * W, *Jy = Jx + (size_t)W * W;
-            const real *p = P + (size_t)n * NN;
-            real *q = Q + (size_t)n * NN;
-            double acc = 0.0;
-            for (int e = threadIdx.x; e < RT_I * RT_J; e += blockDim.x) {
-                const int li = ti * RT_I + e / RT_J, lj = tj * RT_J + (e % RT_J);
-                if (li >= 2 * z || lj >= 2 * z) continue;
-                const int gi = zi0 + li, gj = zj0 + lj;
-                const size_t c = (size_t)gi * N + gj;
-                const int ci = li + 1, cj = lj + 1;   // compact index of the site (ring at 0)
-                real w[3][3];
-                for (int u = 0; u < 3; u++)
-                    for (int v = 0; v < 3; v++) w[u][v] = p[c + (size_t)(u - 1) * N + (v - 1)];
-                const size_t jc = (size_t)ci * W + cj;
-                const real old = w[1][1];
-                const real nv = resh_update<real>(A, B, w, Jx[jc], Jx[jc + W], Jx[jc - W], Jx[jc + 1], Jx[jc - 1],
-                                                  Jy[jc], Jy[jc + W], Jy[jc - W], Jy[jc + 1], Jy[jc - 1], old);
-                q[c] = nv;
-                acc += fabs((double)nv - (double)old) * a.scale;
-            }
-            const double bs = block_sum_d(acc);
-            if (threadIdx.x == 0) {
-                a.part[(size_t)n * a.tpc + tile] = bs;
-                __threadfence();
-                const int ticket = atomicAdd(&a.cnt[n], 1);
-                s_last = (ticket == a.tpc - 1);
-            }
-            __syncthreads();
-            if (s_last && threadIdx.x == 0) {
-                __threadfence();
-                double rdev = 0.0;
-                const volatile double *pp = a.part + (size_t)n * a.tpc;
-                for (int k = 0; k < a.tpc; k++) rdev += pp[k];
-                const int done_iters = a.K[n] + 1;
-                a.K[n] = done_iters;
-                bool stop = false;
-                if (done_iters - 1 > a.rimax) { atomicOr(a.err, ERRBIT_RELAX); stop = true; }
-                if (rdev <= a.thr) stop = true;
-                if (!stop && it == a.cap) { atomicOr(a.err, ERRBIT_ITER_CAP); stop = true; }
-                if (stop) a.done[n] = it;
-                a.cnt[n] = 0;
-            }
-            __syncthreads();
-        }
-        grid.sync();
-        // stamps of the next iteration are > it, so a block that reads late
-        // cannot see a later convergence: every block takes the same decision
-        bool all = true;
-        for (int n = 0; n < a.Ntot && all; n++) {
-            const int d = *(volatile int *)&a.done[n];
-            all = (d != 0 && d <= it);
-        }
-        if (all) break;
-    }
-    // odd iteration counts leave the last iterate in phi; the reference keeps
-    // the penultimate one there (the copy at the top of its loop), which is in phin
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int n = t / a.tpc, tile = t - n * a.tpc;
-        if (!(a.K[n] & 1)) continue;
-        const int ti = tile / a.tiles_j, tj = tile - ti * a.tiles_j;
-        const int zi0 = xc[n] - z, zj0 = yc[n] - z;
-        for (int e = threadIdx.x; e < RT_I * RT_J; e += blockDim.x) {
-            const int li = ti * RT_I + e / RT_J, lj = tj * RT_J + (e % RT_J);
-            if (li >= 2 * z || lj >= 2 * z) continue;
-            const size_t o = (size_t)n * NN + (size_t)(zi0 + li) * N + zj0 + lj;
-            phi[o] = phin[o];
-        }
-    }
-}
-
-// ---- persistent lumen / ECM update + reshaping
-//      (cell_phase_functions.cpp:372-444, :709-871; useful_functions.cpp:422-462)
-struct LumArgs {
-    int N, cap, rimax, npsi;
-    double dx, dt, tau_lum, xi_lum, beta_lum_cells, eta_lum_cells, beta_lum_ECM;
-    double alpha_ECM, tau_ECM, xi_ECM, beta_ECM_cells, eta_ECM_cells;
-    double A, B, thr, rdev0;
-    const double *part_e;
-    double *part;      // [2][gridDim]
-    int *K, *done, *cnt;
-    unsigned *err;
-    double *sum_ecm_out;
-};
-
-template <typename real>
-__device__ __forceinline__ void dirichlet_val(int i, int j, int N, real side, real corner, real &v, bool &edge) {
-    edge = (i == 0 || i == N - 1 || j == 0 || j == N - 1);
-    if (edge) v = ((i == 0 || i == N - 1) && (j == 0 || j == N - 1)) ? corner : side;
-}
-
-template <typename real>
-__global__ void kf_lum(real *__restrict__ lum, real *__restrict__ lumn, real *__restrict__ ecm,
-                       real *__restrict__ ecmn, const real *__restrict__ psi, const real *__restrict__ hl,
-                       const real *__restrict__ he, real *__restrict__ Jl, LumArgs a) {
-    cg::grid_group grid = cg::this_grid();
-    const int N = a.N;
-    const size_t NN = (size_t)N * N;
-    __shared__ double s_sum;
-    __shared__ int s_last, s_skip;
-    // sum_ecm in a fixed order (every block computes the same value)
-    if (threadIdx.x == 0) {
-        double sacc = 0.0;
-        for (int b = 0; b < a.npsi; b++) sacc += a.part_e[b];
-        s_sum = sacc;
-        if (blockIdx.x == 0) *a.sum_ecm_out = sacc;
-    }
-    __syncthreads();
-    const double sum_ecm = s_sum;
-    const real dx = (real)a.dx, dt = (real)a.dt, q4 = (real)4.0 * dx * dx;
-    const real elastic = (real)(a.alpha_ECM * ((double)N * (double)N * a.dx * a.dx - sum_ecm));
-    // phase U: lumn / ECMn (interior), Dirichlet sides (lumen 0, ECM 1, corners as their sides)
-    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < NN; k += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(k / N), j = (int)(k % N);
-        if (i == 0 || i == N - 1 || j == 0 || j == N - 1) { lumn[k] = (real)0.0; ecmn[k] = (real)1.0; continue; }
-        const real s = psi[k];
-        const real L = lap9<real>(s, psi[k + N], psi[k - N], psi[k + 1], psi[k - 1], psi[k + N + 1], psi[k + N - 1],
-                                  psi[k - N - 1], psi[k - N + 1]);
-        const real l = lum[k], e = ecm[k];
-        real ln = l;
-        ln += ((real)1.0 / (real)a.tau_lum) * l * ((real)1.0 - l) * dt *
-              ((real)a.xi_lum - (real)a.beta_lum_cells * s + (real)a.eta_lum_cells * L / q4 -
-               (real)a.beta_lum_ECM * he[k]);
-        real en = e;
-        en += ((real)1.0 / (real)a.tau_ECM) * e * ((real)1.0 - e) * dt *
-              (elastic + (real)a.xi_ECM - (real)a.beta_ECM_cells * s + (real)a.eta_ECM_cells * L / q4 -
-               (real)a.beta_lum_ECM * hl[k]);
-        lumn[k] = ln;
-        ecmn[k] = en;
-    }
-    grid.sync();
-    // phase N: normals J = (1/(2dx)) grad(field_new) / |grad field_old| on every
-    // site, ghost sites through the periodic map (cell_phase_functions.cpp:722-771)
-    const real c4 = (real)(1.0 / a.dx / a.dx / 4.0), inv2dx = (real)(1.0 / (2.0 * a.dx));
-    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < NN; k += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(k / N), j = (int)(k % N);
-        const size_t c = (size_t)ghost_src(i, N) * N + ghost_src(j, N);
-        for (int f = 0; f < 2; f++) {
-            const real *o = f ? ecm : lum;
-            const real *nw = f ? ecmn : lumn;
-            const real ga = o[c + N] - o[c - N], gb = o[c + 1] - o[c - 1];
-            const real g = sqrt(c4 * (ga * ga + gb * gb));
-            Jl[(size_t)(2 * f) * NN + k] = (g != (real)0.0) ? inv2dx * (nw[c + N] - nw[c - N]) / g : (real)0.0;
-            Jl[(size_t)(2 * f + 1) * NN + k] = (g != (real)0.0) ? inv2dx * (nw[c + 1] - nw[c - 1]) / g : (real)0.0;
-        }
-    }
-    grid.sync();
-    // phase R: relaxation loops of both fields, iteration k reads P, writes Q
-    const real A = (real)a.A, B = (real)a.B;
-    const double dx2 = a.dx * a.dx;
-    for (int it = 1; it <= a.cap; it++) {
-        for (int f = 0; f < 2; f++) {
-            if (threadIdx.x == 0) {
-                const int d = *(volatile int *)&a.done[f];
-                s_skip = (d != 0 && d < it);
-            }
-            __syncthreads();
-            const bool skip = s_skip;
-            __syncthreads();
-            if (skip) continue;
-            real *P = (it & 1) ? (f ? ecmn : lumn) : (f ? ecm : lum);
-            real *Q = (it & 1) ? (f ? ecm : lum) : (f ? ecmn : lumn);
-            const real side = f ? (real)1.0 : (real)0.0;
-            const real *Jx = Jl + (size_t)(2 * f) * NN, *Jy = Jl + (size_t)(2 * f + 1) * NN;
-            double acc = 0.0;
-            for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < NN; k += (size_t)gridDim.x * blockDim.x) {
-                const int i = (int)(k / N), j = (int)(k % N);
-                real v;
-                bool edge;
-                dirichlet_val<real>(i, j, N, side, (real)0.0, v, edge);
-                if (!edge) {
-                    real w[3][3];
-                    for (int u = 0; u < 3; u++)
-                        for (int q = 0; q < 3; q++) w[u][q] = P[k + (size_t)(u - 1) * N + (q - 1)];
-                    v = resh_update<real>(A, B, w, Jx[k], Jx[k + N], Jx[k - N], Jx[k + 1], Jx[k - 1], Jy[k],
-                                          Jy[k + N], Jy[k - N], Jy[k + 1], Jy[k - 1], w[1][1]);
-                }
-                acc += fabs((double)v - (double)P[k]) * dx2;
-                Q[k] = v;
-            }
-            const double bs = block_sum_d(acc);
-            if (threadIdx.x == 0) {
-                a.part[(size_t)f * gridDim.x + blockIdx.x] = bs;
-                __threadfence();
-                const int ticket = atomicAdd(&a.cnt[f], 1);
-                s_last = (ticket == (int)gridDim.x - 1);
-            }
-            __syncthreads();
-            if (s_last && threadIdx.x == 0) {
-                __threadfence();
-                double rdev = 0.0;
-                const volatile double *pp = a.part + (size_t)f * gridDim.x;
-                for (int b = 0; b < (int)gridDim.x; b++) rdev += pp[b];
-                const int k2 = a.K[f] + 1;
-                a.K[f] = k2;
-                bool stop = false;
-                if (k2 - 1 > a.rimax) { atomicOr(a.err, ERRBIT_RELAX); stop = true; }
-                if (rdev <= a.thr) stop = true;
-                if (!stop && it == a.cap) { atomicOr(a.err, ERRBIT_ITER_CAP); stop = true; }
-                if (stop) a.done[f] = it;
-                a.cnt[f] = 0;
-            }
-            __syncthreads();
-        }
-        grid.sync();
-        const int d0 = *(volatile int *)&a.done[0], d1 = *(volatile int *)&a.done[1];
-        if (d0 != 0 && d0 <= it && d1 != 0 && d1 <= it) break;
-    }
-    // the step ends with lum <- lumn: the last iterate is in lum for odd counts
-    for (int f = 0; f < 2; f++) {
-        if (a.K[f] & 1) continue;
-        real *dst = f ? ecm : lum;
-        const real *src = f ? ecmn : lumn;
-        for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < NN; k += (size_t)gridDim.x * blockDim.x)
-            dst[k] = src[k];
-    }
-}
-
-// ---- end of step: rho <- rhon on the boxes, then the periodic ghost ring
-template <typename real>
-__global__ void kf_rho_copy(real *__restrict__ rho, const real *__restrict__ rhon, const int *__restrict__ xc,
-                            const int *__restrict__ yc, int N, int z, int M) {
-    const int n = blockIdx.z;
-    const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= M || j >= M) return;
-    const size_t o = (size_t)n * N * N + (size_t)(xc[n] - z + 1 + i) * N + (yc[n] - z + 1 + j);
-    rho[o] = rhon[o];
-}
-
-template <typename real>
-__global__ void kf_rho_ring(real *__restrict__ rho, int N) {
-    const int n = blockIdx.y;
-    real *p = rho + (size_t)n * N * N;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < 4 * N; k += gridDim.x * blockDim.x) {
-        int i, j;
-        if (k < N) { i = 0; j = k; }
-        else if (k < 2 * N) { i = N - 1; j = k - N; }
-        else if (k < 3 * N) { i = k - 2 * N; j = 0; }
-        else { i = k - 3 * N; j = N - 1; }
-        if ((k >= 2 * N) && (i == 0 || i == N - 1)) continue;
-        p[(size_t)i * N + j] = p[(size_t)ghost_src(i, N) * N + ghost_src(j, N)];
-    }
-}
-
-// upload: initial support rectangles and the exactness precondition
-template <typename real>
-__global__ void kf_outside_check(const real *__restrict__ phi, const int4 *__restrict__ rect, int N,
-                                 unsigned *__restrict__ bad) {
-    const int n = blockIdx.y;
-    const int4 r = rect[n];
-    const real *p = phi + (size_t)n * N * N;
-    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < (size_t)N * N; k += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(k / N), j = (int)(k % N);
-        if (i >= r.x && i < r.y && j >= r.z && j < r.w) continue;
-        if (p[k] > (real)0.5) atomicOr(bad, 1u);
-    }
-}
-
-__global__ void kf_rect_init(int4 *rect, int Ntot, int N) {
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n < Ntot) rect[n] = make_int4(N, 0, N, 0);   // empty; the first centroid sets it to the zone
-}
-
-// ---------------------------------------------------------------------------
-FusedRes *F(pfag_ctx *c) { return (FusedRes *)c->fused; }
-
-BoxArgs box_args(pfag_ctx *c) {
-    BoxArgs a{};
-    const DevParams &d = c->dp;
-    a.N = c->N; a.z = c->zone; a.M = c->M; a.logm = F(c)->logm; a.Ntot = c->Ntot;
-    a.c4 = 1.0 / d.dx / d.dx / 4.0; a.sigma = d.sigma; a.dt = d.dt; a.kfac = d.kfac; a.friction = d.friction;
-    a.dx = d.dx;
-    for (int k = 0; k < 3; k++) {
-        a.deg[k] = d.deg[k]; a.gen[k] = d.gen[k]; a.a_ort[k] = d.a_ort[k]; a.a_tan[k] = d.a_tan[k];
-        a.visc[k] = d.visc[k]; a.bb[k] = d.bb[k];
-    }
-    return a;
-}
-
-template <typename real>
-int launch_coop(const void *fn, int blocks, void **args, size_t smem, cudaStream_t s) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(blocks);
-    cfg.blockDim = dim3(FT);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    PFAG_CUDA_CHECK(cudaLaunchKernelExC(&cfg, fn, args));
-    return PFAG_OK;
-}
-
-template <typename real>
-struct Fused {
-    typedef typename Cplx<real>::type cx;
-    pfag_ctx *c;
-    FusedRes *r;
-    explicit Fused(pfag_ctx *ctx) : c(ctx), r(F(ctx)) {}
-    real *R(void *p) { return (real *)p; }
-
-    int configure() {
-        const int M = c->M;
-        int logm = 0;
-        while ((1 << logm) < M) logm++;
-        if ((1 << logm) != M || M < 16 || M > 1024) {
-            pfag_set_error("fused path needs a power-of-two FFT box (2*zone_size-2 = %d); use the plain path", M);
-            return PFAG_E_UNSUPPORTED;
-        }
-        if (c->Ntot > 1024) { pfag_set_error("fused path supports at most 1024 cells"); return PFAG_E_UNSUPPORTED; }
-        r->logm = logm;
-        const size_t cs = sizeof(cx);
-        // rows per block for the row passes: keep the shared tile near 64 KB
-        int R = std::max(1, std::min(8, (int)(65536 / (2 * (size_t)M * cs))));
-        R = std::min(R, std::max(1, 8 * FT / M));   // pass C keeps <= 8 elements per thread in registers
-        while (M % R) R--;
-        r->rows_blk = R;
-        int G = std::max(1, std::min(16, (int)(98304 / (4 * (size_t)(M + 1) * cs))));
-        r->grp_cols = G;
-        r->smemA = (M + 2 * (size_t)R * M) * cs;
-        r->smemC = (M + (size_t)R * M) * cs;
-        r->smemE = r->smemC;
-        r->smemB = (M + 2 * 2 * (size_t)G * (M + 1)) * cs;
-        r->smemD = (M + 2 * (size_t)G * (M + 1)) * cs;
-        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_boxA<real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smemA));
-        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_boxB<real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smemB));
-        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_boxC<real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smemC));
-        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_boxD<real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smemD));
-        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_boxE<real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smemE));
-        int dev = 0, nsm = 0, per = 0;
-        PFAG_CUDA_CHECK(cudaGetDevice(&dev));
-        PFAG_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kf_reshape<real>, FT, 0));
-        r->coop_r = std::max(1, nsm * std::min(per, 4));
-        PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kf_lum<real>, FT, 0));
-        r->coop_l = std::max(1, nsm * std::min(per, 4));
-        r->tiles_i = (2 * c->zone + RT_I - 1) / RT_I;
-        r->tiles_j = (2 * c->zone + RT_J - 1) / RT_J;
-        r->tpc = r->tiles_i * r->tiles_j;
-        r->npsi = ((c->N + 31) / 32) * ((c->N + 31) / 32);
-        return PFAG_OK;
-    }
-
-    int alloc() {
-        PFAG_TRY(configure());
-        const size_t mm = (size_t)c->M * c->M, rs = c->rsz, W = 2 * c->zone + 2;
-        PFAG_CUDA_CHECK(cudaMalloc(&r->Y1, (size_t)c->Ntot * mm * 2 * rs));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->Y2, (size_t)c->Ntot * mm * 2 * rs));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->Rb, (size_t)c->Ntot * mm * rs));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->clsT, (size_t)c->Ntot * mm));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->Jc, (size_t)c->Ntot * 2 * W * W * rs));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->Jl, 4 * c->ng * rs));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->rect, sizeof(int4) * c->Ntot));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->part_s, sizeof(double) * c->Ntot * SBLK));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->part_r, sizeof(double) * (size_t)c->Ntot * r->tpc));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->part_e, sizeof(double) * r->npsi));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->part_l, sizeof(double) * 2 * r->coop_l));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->cK, sizeof(int) * (3 * c->Ntot + 8)));
-        r->cdone = r->cK + c->Ntot;
-        r->ccnt = r->cK + 2 * c->Ntot;
-        r->lK = r->cK + 3 * c->Ntot;
-        r->ldone = r->lK + 2;
-        r->lcnt = r->lK + 4;
-        PFAG_CUDA_CHECK(cudaMemset(r->cK, 0, sizeof(int) * (3 * c->Ntot + 8)));
-        return PFAG_OK;
-    }
-
-    int upload_hook() {
-        // full-grid centroid of the initial state, first support rectangle = first zone
-        kf_rect_init<<<(c->Ntot + 127) / 128, 128, 0, c->stream>>>(r->rect, c->Ntot, c->N);
-        PFAG_CUDA_CHECK(cudaMemsetAsync(c->d_cacc, 0, sizeof(long long) * 3 * c->Ntot, c->stream));
-        int4 full = make_int4(0, c->N, 0, c->N);
-        std::vector<int4> hf(c->Ntot, full);
-        int4 *tmp = nullptr;
-        PFAG_CUDA_CHECK(cudaMalloc(&tmp, sizeof(int4) * c->Ntot));
-        PFAG_CUDA_CHECK(cudaMemcpyAsync(tmp, hf.data(), sizeof(int4) * c->Ntot, cudaMemcpyHostToDevice, c->stream));
-        kf_centroid<real><<<dim3(64, c->Ntot), FT, 0, c->stream>>>(R(c->phi), tmp, c->N, c->d_cacc);
-        kf_centroid_finalize<<<(c->Ntot + 127) / 128, 128, 0, c->stream>>>(c->d_cacc, c->Ntot, c->N, c->zone, c->d_xc,
-                                                                           c->d_yc, r->rect, c->d_err);
-        PFAG_CUDA_CHECK(cudaMemsetAsync(c->d_err + 1, 0, sizeof(unsigned), c->stream));
-        kf_outside_check<real><<<dim3(64, c->Ntot), FT, 0, c->stream>>>(R(c->phi), r->rect, c->N, c->d_err + 1);
-        PFAG_CUDA_CHECK(cudaMemcpyAsync(c->h_err, c->d_err, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
-        PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
-        cudaFree(tmp);
-        PFAG_CUDA_CHECK(cudaGetLastError());
-        if (c->h_err[1]) {
-            pfag_set_error("fused path precondition: a cell has phi > 0.5 outside its first zone; use the plain path");
-            return PFAG_E_UNSUPPORTED;
-        }
-        if (c->h_err[0]) {
-            PFAG_CUDA_CHECK(cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), c->stream));
-            pfag_set_error("initial zone leaves the grid or a cell is empty");
-            return (c->h_err[0] & ERRBIT_EMPTY_CELL) ? PFAG_E_EMPTY_CELL : PFAG_E_ZONE;
-        }
-        r->graph_ok = false;
-        return PFAG_OK;
-    }
-
-    // enqueue one step (no host synchronisation; capturable)
-    int enqueue() {
-        cudaStream_t s = c->stream;
-        const int N = c->N, Nt = c->Ntot, M = c->M, z = c->zone;
-        const DevParams &d = c->dp;
-        // 1. centroids over B_n
-        PFAG_CUDA_CHECK(cudaMemsetAsync(c->d_cacc, 0, sizeof(long long) * 3 * Nt, s));
-        kf_centroid<real><<<dim3(SBLK, Nt), FT, 0, s>>>(R(c->phi), r->rect, N, c->d_cacc); PFAG_LAUNCHED(c);
-        kf_centroid_finalize<<<(Nt + 127) / 128, 128, 0, s>>>(c->d_cacc, Nt, N, z, c->d_xc, c->d_yc, r->rect,
-                                                               c->d_err);
-        PFAG_LAUNCHED(c);
-        // 2. hfunc on the zones, areas over B_n
-        kf_hfunc_area<real><<<dim3(SBLK, Nt), FT, 0, s>>>(R(c->phi), R(c->hfunc), c->d_xc, c->d_yc, r->rect, N, z,
-                                                          d.dx * d.dx, r->part_s);
-        PFAG_LAUNCHED(c);
-        kf_area_finalize<<<(Nt + 127) / 128, 128, 0, s>>>(r->part_s, SBLK, Nt, d.alpha, d.s0, c->d_s, c->d_f0);
-        PFAG_LAUNCHED(c);
-        // 3. psi, h(lum), h(ECM), sum_ecm partials
-        const int tiles = (N + 31) / 32;
-        kf_psi<real><<<dim3(tiles, tiles), FT, 0, s>>>(R(c->hfunc), r->rect, Nt, N, R(c->lum), R(c->ecm), R(c->psi),
-                                                        R(c->hlum), R(c->hecm), d.dx * d.dx, r->part_e);
-        PFAG_LAUNCHED(c);
-        // 4. spectral solve
-        const BoxArgs ba = box_args(c);
-        const int Rr = r->rows_blk, G = r->grp_cols;
-        cx *Y1 = (cx *)r->Y1, *Y2 = (cx *)r->Y2;
-        kf_boxA<real><<<dim3(M / Rr, Nt), FT, r->smemA, s>>>(R(c->phi), R(c->rho), R(c->lum), R(c->ecm), c->d_xc,
-                                                             c->d_yc, ba, Rr, Y1, Y2, R(r->Rb), r->clsT);
-        PFAG_LAUNCHED(c);
-        const int ngrp = (M / 2 + 1 + G - 1) / G;
-        kf_boxB<real><<<dim3(ngrp, Nt), FT, r->smemB, s>>>(Y1, Y2, r->clsT, ba, G); PFAG_LAUNCHED(c);
-        kf_boxC<real><<<dim3(M / Rr, Nt), FT, r->smemC, s>>>(Y1, Y2, R(c->rho), c->d_xc, c->d_yc, ba, Rr,
-                                                             c->debug ? R(c->d_vx) : nullptr,
-                                                             c->debug ? R(c->d_vy) : nullptr);
-        PFAG_LAUNCHED(c);
-        kf_boxD<real><<<dim3(ngrp, Nt), FT, r->smemD, s>>>(Y1, Y2, ba, G); PFAG_LAUNCHED(c);
-        kf_boxE<real><<<dim3(M / Rr, Nt), FT, r->smemE, s>>>(Y1, R(c->rho), R(r->Rb), R(c->rhon), c->d_xc, c->d_yc,
-                                                             ba, Rr);
-        PFAG_LAUNCHED(c);
-        // 5. lumen / ECM
-        PFAG_CUDA_CHECK(cudaMemsetAsync(r->lK, 0, sizeof(int) * 8, s));
-        {
-            LumArgs la{};
-            la.N = N; la.rimax = c->p.rimax; la.cap = c->relax_cap; la.npsi = r->npsi;
-            la.dx = d.dx; la.dt = d.dt; la.tau_lum = d.tau_lum; la.xi_lum = d.xi_lum;
-            la.beta_lum_cells = d.beta_lum_cells; la.eta_lum_cells = d.eta_lum_cells; la.beta_lum_ECM = d.beta_lum_ECM;
-            la.alpha_ECM = d.alpha_ECM; la.tau_ECM = d.tau_ECM; la.xi_ECM = d.xi_ECM;
-            la.beta_ECM_cells = d.beta_ECM_cells; la.eta_ECM_cells = d.eta_ECM_cells;
-            la.A = d.A_resh; la.B = d.B_resh; la.thr = d.thr_lum; la.rdev0 = d.rdev0_lum;
-            la.part_e = r->part_e; la.part = r->part_l; la.K = r->lK; la.done = r->ldone; la.cnt = r->lcnt;
-            la.err = c->d_err; la.sum_ecm_out = c->d_scal + 0;
-            real *a0 = R(c->lum), *a1 = R(c->lumn), *a2 = R(c->ecm), *a3 = R(c->ecmn), *a5 = R(c->hlum),
-                 *a6 = R(c->hecm), *a7 = R(r->Jl);
-            const real *a4 = R(c->psi);
-            const real *a5c = a5, *a6c = a6;
-            void *args[] = {&a0, &a1, &a2, &a3, (void *)&a4, (void *)&a5c, (void *)&a6c, &a7, &la};
-            PFAG_TRY(launch_coop<real>((const void *)kf_lum<real>, r->coop_l, args, 0, s));
-            PFAG_LAUNCHED(c);
-        }
-        // 6. phi update + normals, then reshaping
-        {
-            const int W = 2 * z + 2;
-            dim3 tb(32, 8), gb((W + 31) / 32, (W + 7) / 8, Nt);
-            kf_update<real><<<gb, tb, 0, s>>>(R(c->phi), R(c->phin), R(c->rho), R(c->hfunc), c->d_f0, R(c->psi),
-                                              R(c->hlum), R(c->hecm), c->d_xc, c->d_yc, c->dp, R(r->Jc));
-            PFAG_LAUNCHED(c);
-        }
-        PFAG_CUDA_CHECK(cudaMemsetAsync(r->cK, 0, sizeof(int) * 3 * Nt, s));
-        {
-            ReshArgs ra{};
-            ra.N = N; ra.z = z; ra.Ntot = Nt; ra.tpc = r->tpc; ra.tiles_i = r->tiles_i; ra.tiles_j = r->tiles_j;
-            ra.rimax = c->p.rimax; ra.cap = c->relax_cap;
-            ra.A = d.A_resh; ra.B = d.B_resh; ra.scale = d.dx * d.dx / (double)d.Ncur; ra.thr = d.thr_cells;
-            ra.K = r->cK; ra.done = r->cdone; ra.cnt = r->ccnt; ra.part = r->part_r; ra.err = c->d_err;
-            real *a0 = R(c->phi), *a1 = R(c->phin);
-            const real *a2 = R(r->Jc);
-            const int *a3 = c->d_xc, *a4 = c->d_yc;
-            void *args[] = {&a0, &a1, (void *)&a2, (void *)&a3, (void *)&a4, &ra};
-            PFAG_TRY(launch_coop<real>((const void *)kf_reshape<real>, r->coop_r, args, 0, s));
-            PFAG_LAUNCHED(c);
-        }
-        // 7. rho <- rhon on the boxes, ghost ring
-        {
-            dim3 tb(32, 8), gb((M + 31) / 32, (M + 7) / 8, Nt);
-            kf_rho_copy<real><<<gb, tb, 0, s>>>(R(c->rho), R(c->rhon), c->d_xc, c->d_yc, N, z, M); PFAG_LAUNCHED(c);
-            kf_rho_ring<real><<<dim3((4 * N + 255) / 256, Nt), 256, 0, s>>>(R(c->rho), N); PFAG_LAUNCHED(c);
-        }
-        PFAG_CUDA_CHECK(cudaGetLastError());
-        return PFAG_OK;
-    }
-
-    int stats() {
-        const int Nt = c->Ntot;
-        std::vector<int> h(3 * Nt + 8);
-        PFAG_CUDA_CHECK(cudaMemcpyAsync(h.data(), r->cK, sizeof(int) * (3 * Nt + 8), cudaMemcpyDeviceToHost, c->stream));
-        PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
-        int mx = 0, sm = 0;
-        for (int n = 0; n < Nt; n++) {
-            c->h_iflags[4 * Nt + n] = h[n];
-            mx = std::max(mx, h[n]);
-            sm += h[n];
-        }
-        c->stats.cell_iters_max = mx;
-        c->stats.cell_iters_sum = sm;
-        c->stats.lum_iters = h[3 * Nt + 0];
-        c->stats.ecm_iters = h[3 * Nt + 1];
-        return PFAG_OK;
-    }
-};
-
-}  // namespace
+int pfag_fused_alloc_f64(pfag_ctx *c);
+int pfag_fused_alloc_f32(pfag_ctx *c);
+int pfag_fused_upload_f64(pfag_ctx *c);
+int pfag_fused_upload_f32(pfag_ctx *c);
+int pfag_fused_step_f64(pfag_ctx *c, bool sync_host);
+int pfag_fused_step_f32(pfag_ctx *c, bool sync_host);
 
 int pfag_fused_alloc(pfag_ctx *c) {
     c->fused = new FusedRes();
     std::memset(c->fused, 0, sizeof(FusedRes));
-    return c->prec == 64 ? Fused<double>(c).alloc() : Fused<float>(c).alloc();
+    return c->prec == 64 ? pfag_fused_alloc_f64(c) : pfag_fused_alloc_f32(c);
 }
 
 void pfag_fused_free(pfag_ctx *c) {
@@ -1181,16 +28,9 @@ void pfag_fused_free(pfag_ctx *c) {
 }
 
 int pfag_fused_upload_hook(pfag_ctx *c) {
-    return c->prec == 64 ? Fused<double>(c).upload_hook() : Fused<float>(c).upload_hook();
+    return c->prec == 64 ? pfag_fused_upload_f64(c) : pfag_fused_upload_f32(c);
 }
 
-int pfag_fused_step(pfag_ctx *c, int it, bool sync_host) {
-    (void)it;
-    int rc = c->prec == 64 ? Fused<double>(c).enqueue() : Fused<float>(c).enqueue();
-    if (rc != PFAG_OK) return rc;
-    if (sync_host) {
-        PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
-        rc = c->prec == 64 ? Fused<double>(c).stats() : Fused<float>(c).stats();
-    }
-    return rc;
+int pfag_fused_step(pfag_ctx *c, int, bool sync_host) {
+    return c->prec == 64 ? pfag_fused_step_f64(c, sync_host) : pfag_fused_step_f32(c, sync_host);
 }

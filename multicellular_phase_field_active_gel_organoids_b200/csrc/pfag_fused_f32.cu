@@ -1,0 +1,6 @@
+// FP32 instantiation of the fused path (kernels in pfag_fused_impl.cuh).
+#include "pfag_fused_impl.cuh"
+
+int pfag_fused_alloc_f32(pfag_ctx *c) { return fused_alloc_t<float>(c); }
+int pfag_fused_upload_f32(pfag_ctx *c) { return fused_upload_t<float>(c); }
+int pfag_fused_step_f32(pfag_ctx *c, bool sync_host) { return fused_step_t<float>(c, sync_host); }

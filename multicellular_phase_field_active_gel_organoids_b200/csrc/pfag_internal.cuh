@@ -105,10 +105,15 @@ struct pfag_ctx {
     void *d_vx, *d_vy;
     // fused-path resources (opaque, owned by pfag_fused.cu)
     void *fused;
+    void *prof;           // per-kernel event timing (pfag_prof.cu)
 };
 
-// Launch accounting helper.
-#define PFAG_LAUNCHED(ctx) ((ctx)->launches++)
+void pfag_prof_begin(pfag_ctx *ctx, const char *name);
+void pfag_prof_end(pfag_ctx *ctx);
+void pfag_prof_free(pfag_ctx *ctx);
+
+// Launch accounting helper; closes the profiling bracket of the launch.
+#define PFAG_LAUNCHED(ctx) ((ctx)->launches++, pfag_prof_end(ctx))
 
 int pfag_plain_alloc(pfag_ctx *ctx);
 void pfag_plain_free(pfag_ctx *ctx);
