@@ -140,6 +140,27 @@ int pfag_fn_compute_normal_to_phi(pfag_ctx *ctx);              /* useful_functio
 int pfag_fn_update_all_cells(pfag_ctx *ctx);                   /* cell_phase_functions.cpp:126-217 + useful_functions.cpp:391-420 */
 int pfag_fn_reshaping_cells(pfag_ctx *ctx);                    /* cell_phase_functions.cpp:447-580 */
 int pfag_fn_copy_back(pfag_ctx *ctx);                          /* run_with_active_gels.cpp:175-182 */
+/* Cell areas s[n] = sum of hfunc_cell[n] dx^2 over the grid and
+ * f0[n] = alpha (s0 - s[n]), computed the way pfag_fn_sum_s_kernels computes
+ * them, for callers that cannot allocate device memory: a host program whose
+ * device memory already belongs to another allocator (an OpenACC data region,
+ * a framework's caching allocator, a pool reserved up front), or a
+ * latency-critical loop that must not pay cudaMalloc's device
+ * synchronisation.  This entry point has no counterpart in the reference.
+ * It allocates nothing: its scratch is a 1 MiB static device array that each
+ * GPU loading the library holds until exit, so Ntot may be at most 1024
+ * (larger values return PFAG_E_ARG).  hfunc_cell ([Ntot][N_s][N_s], element
+ * type by precision 32/64), s and f0 (Ntot doubles) are device pointers the
+ * caller owns; the work is enqueued on `stream` (a cudaStream_t, NULL for the
+ * default stream) and not synchronised.  The first call on a device resolves
+ * the scratch address there (cudaGetSymbolAddress) and should be made before
+ * any stream capture.  All calls share the one scratch array, so calls that
+ * overlap on the GPU (different streams, no ordering) race; order them on one
+ * stream.  Every scratch value a call reads it first writes, so no clearing
+ * is needed between calls. */
+int pfag_areas_noalloc(const void *hfunc_cell, int precision, int Ntot, int N_s, double dx, double alpha,
+                       double s0, double *s, double *f0, void *stream);
+
 /* saving_out_functions (useful_functions.cpp:66-99): device state -> host
  * snapshot slot; phi_out/rho_out get Ntot*N*N, lum_out/ecm_out N*N elements. */
 int pfag_fn_saving_out_functions(pfag_ctx *ctx, void *phi_out, void *rho_out, void *lum_out, void *ecm_out);
