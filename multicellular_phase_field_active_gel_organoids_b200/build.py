@@ -45,8 +45,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return LIB
     os.makedirs(OBJ_DIR, exist_ok=True)
-    objs = []
-    for src in sources():
+
+    def compile_one(src):
         obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
         cmd = [NVCC, *ARCH, *FLAGS, *PER_FILE.get(os.path.basename(src), []), "-c", src, "-o", obj]
         if verbose:
@@ -56,7 +56,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
             raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
         if verbose:
             sys.stderr.write(r.stderr)
-        objs.append(obj)
+        return obj
+
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        objs = list(ex.map(compile_one, sources()))
     cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcufft", "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
