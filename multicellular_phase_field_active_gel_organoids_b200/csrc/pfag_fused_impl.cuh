@@ -27,6 +27,7 @@
 #pragma once
 #include "pfag_internal.cuh"
 #include "pfag_fft.cuh"
+#include "pfag_regfft.cuh"
 #include <cooperative_groups.h>
 #include <algorithm>
 #include <cmath>
@@ -569,6 +570,311 @@ __global__ void kf_boxE(const typename Cplx<real>::type *__restrict__ Y1, const 
     }
 }
 
+// ---- box passes on register-resident FFTs (M = 32 .. 256) ----------------
+template <int M> struct BoxGeom {
+    static constexpr int TT = RegFFT<float2, M>::TT;          // threads per transform
+    static constexpr int ROWS = (256 / TT < M) ? 256 / TT : M; // rows per block of the row passes
+    static constexpr int THREADS = TT * ROWS;
+    static constexpr int WG = 32 / TT;                       // thread groups per warp
+};
+
+// Pass A on register FFTs: one thread group per box row.
+template <typename real, int M>
+__global__ void __launch_bounds__(256) kr_boxA(const real *__restrict__ phi, const real *__restrict__ rho,
+                                               const real *__restrict__ lum, const real *__restrict__ ecm,
+                                               const int *__restrict__ xc, const int *__restrict__ yc, BoxArgs a,
+                                               typename Cplx<real>::type *__restrict__ Y1,
+                                               typename Cplx<real>::type *__restrict__ Y2, real *__restrict__ Rb,
+                                               unsigned char *__restrict__ clsT) {
+    typedef typename Cplx<real>::type cx;
+    typedef RegFFT<cx, M> RF;
+    constexpr int TT = RF::TT, E1 = RF::E1, ROWS = BoxGeom<M>::ROWS;
+    extern __shared__ unsigned char smraw[];
+    cx *tw = (cx *)smraw;
+    cx *scr = tw + M;                                   // [ROWS][M] exchange scratch
+    real *xys = (real *)(scr + ROWS * M);               // [ROWS][M] pi_xy, read back by the same thread
+    unsigned char *cls = (unsigned char *)(xys + ROWS * M);  // [ROWS][M]
+    fft_twiddles(tw, M);
+    __syncthreads();
+    const int t = threadIdx.x % TT, g = threadIdx.x / TT;
+    const int n = blockIdx.y, i0 = blockIdx.x * ROWS, i = i0 + g;
+    const int N = a.N;
+    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
+    const int n1 = (n == 0) ? a.Ntot - 1 : n - 1;
+    const int n2 = (n == a.Ntot - 1) ? 0 : n + 1;
+    const size_t NN = (size_t)N * N;
+    const real *p = phi + (size_t)n * NN;
+    const real c4 = (real)a.c4, sigma = (real)a.sigma;
+    const size_t rowo = ((size_t)n * M + i) * M;
+    cx v[E1];
+#pragma unroll
+    for (int q = 0; q < E1; q++) {
+        const int j = RF::in_index(t, q);
+        const size_t s = (size_t)(bi + i) * N + (bj + j);
+        const real f = p[s];
+        const real dxp = p[s + N] - p[s - N];
+        const real dyp = p[s + 1] - p[s - 1];
+        const real gg = sqrt(c4 * (dxp * dxp + dyp * dyp));
+        const int c = map_class_f<real>(f, lum[s], ecm[s], phi[(size_t)n1 * NN + s], phi[(size_t)n2 * NN + s]);
+        const real rr = rho[(size_t)n * NN + s];
+        const real at = (real)a.a_tan[c], ao = (real)a.a_ort[c], b = (real)a.bb[c];
+        real xx = -at * rr * rr * rr + b * rr * rr * rr * rr;
+        real yy = xx, xy = (real)0.0;
+        if (gg > (real)0.0) {
+            xx += (at - ao) * rr * rr * rr * c4 * dxp * dxp / gg / gg;
+            yy += (at - ao) * rr * rr * rr * c4 * dyp * dyp / gg / gg;
+            xy += (at - ao) * rr * rr * rr * c4 * dxp * dyp / gg / gg;
+        }
+        const real P = gg * exp(-(f - (real)0.5) * (f - (real)0.5) / (real)2.0 / sigma / sigma) /
+                       sqrt((real)(2.0 * M_PI)) / sigma;
+        Rb[rowo + j] = -(real)a.deg[c] * rr + (real)a.gen[c] * P;
+        cls[g * M + j] = (unsigned char)c;
+        xys[g * M + j] = xy;
+        v[q].x = xx;
+        v[q].y = yy;
+    }
+    RF::template run<false>(v, t, scr + g * M, tw);
+#pragma unroll
+    for (int r = 0; r < RF::R2; r++)
+#pragma unroll
+        for (int k2 = 0; k2 < TT; k2++) Y1[rowo + RF::out_index(t, r, k2)] = v[r * TT + k2];
+#pragma unroll
+    for (int q = 0; q < E1; q++) {
+        v[q].x = xys[g * M + RF::in_index(t, q)];
+        v[q].y = (real)0.0;
+    }
+    RF::template run<false>(v, t, scr + g * M, tw);
+#pragma unroll
+    for (int r = 0; r < RF::R2; r++)
+#pragma unroll
+        for (int k2 = 0; k2 < TT; k2++) Y2[rowo + RF::out_index(t, r, k2)] = v[r * TT + k2];
+    __syncthreads();
+    // class map transposed, ROWS consecutive bytes per column
+    for (int e = threadIdx.x; e < M * ROWS; e += blockDim.x) {
+        const int j = e / ROWS, r = e % ROWS;
+        clsT[((size_t)n * M + j) * M + i0 + r] = cls[r * M + j];
+    }
+}
+
+// Pass C on register FFTs.
+template <typename real, int M>
+__global__ void __launch_bounds__(256) kr_boxC(const typename Cplx<real>::type *__restrict__ Y1,
+                                               typename Cplx<real>::type *__restrict__ Y2,
+                                               const real *__restrict__ rho, const int *__restrict__ xc,
+                                               const int *__restrict__ yc, BoxArgs a, real *__restrict__ vdx,
+                                               real *__restrict__ vdy) {
+    typedef typename Cplx<real>::type cx;
+    typedef RegFFT<cx, M> RF;
+    constexpr int TT = RF::TT, E1 = RF::E1, ROWS = BoxGeom<M>::ROWS;
+    extern __shared__ unsigned char smraw[];
+    cx *tw = (cx *)smraw;
+    cx *scr = tw + M;
+    fft_twiddles(tw, M);
+    __syncthreads();
+    const int t = threadIdx.x % TT, g = threadIdx.x / TT;
+    const int n = blockIdx.y, i = blockIdx.x * ROWS + g;
+    const int N = a.N;
+    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
+    const size_t rowo = ((size_t)n * M + i) * M;
+    cx *sm = scr + g * M;
+    cx v[E1];
+#pragma unroll
+    for (int q = 0; q < E1; q++) v[q] = Y1[rowo + RF::in_index(t, q)];
+    RF::template run<true>(v, t, sm, tw);
+    const real mm = (real)((double)M * (double)M);
+    const real *rh = rho + (size_t)n * N * N + (size_t)(bi + i) * N + bj;
+#pragma unroll
+    for (int r = 0; r < RF::R2; r++)
+#pragma unroll
+        for (int k2 = 0; k2 < TT; k2++) {
+            const int k = RF::out_index(t, r, k2);
+            const cx val = v[r * TT + k2];
+            const real rr = rh[k];
+            cx qv;
+            qv.x = rr * val.x / mm;     // load_fft_rho_v, rho_functions.cpp:279
+            qv.y = rr * val.y / mm;
+            if (vdx) { vdx[rowo + k] = val.x / mm; vdy[rowo + k] = val.y / mm; }
+            sm[k] = qv;
+        }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < E1; q++) v[q] = sm[RF::in_index(t, q)];
+    __syncwarp();
+    RF::template run<false>(v, t, sm, tw);
+#pragma unroll
+    for (int r = 0; r < RF::R2; r++)
+#pragma unroll
+        for (int k2 = 0; k2 < TT; k2++) Y2[rowo + RF::out_index(t, r, k2)] = v[r * TT + k2];
+}
+
+// Pass E on register FFTs.
+template <typename real, int M>
+__global__ void __launch_bounds__(256) kr_boxE(const typename Cplx<real>::type *__restrict__ Y1,
+                                               const real *__restrict__ rho, const real *__restrict__ Rb,
+                                               real *__restrict__ rhon, const int *__restrict__ xc,
+                                               const int *__restrict__ yc, BoxArgs a) {
+    typedef typename Cplx<real>::type cx;
+    typedef RegFFT<cx, M> RF;
+    constexpr int TT = RF::TT, E1 = RF::E1, ROWS = BoxGeom<M>::ROWS;
+    extern __shared__ unsigned char smraw[];
+    cx *tw = (cx *)smraw;
+    cx *scr = tw + M;
+    fft_twiddles(tw, M);
+    __syncthreads();
+    const int t = threadIdx.x % TT, g = threadIdx.x / TT;
+    const int n = blockIdx.y, i = blockIdx.x * ROWS + g;
+    const int N = a.N;
+    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
+    const size_t rowo = ((size_t)n * M + i) * M;
+    cx v[E1];
+#pragma unroll
+    for (int q = 0; q < E1; q++) v[q] = Y1[rowo + RF::in_index(t, q)];
+    RF::template run<true>(v, t, scr + g * M, tw);
+    const real mm = (real)((double)M * (double)M), dt = (real)a.dt;
+    const size_t so = (size_t)n * N * N + (size_t)(bi + i) * N + bj;
+#pragma unroll
+    for (int r = 0; r < RF::R2; r++)
+#pragma unroll
+        for (int k2 = 0; k2 < TT; k2++) {
+            const int k = RF::out_index(t, r, k2);
+            rhon[so + k] = rho[so + k] + dt * Rb[rowo + k] + v[r * TT + k2].x / mm;
+        }
+}
+
+// Column transforms of the slots held in shared memory (natural order in and
+// out); each column's own storage is the exchange scratch of its transform.
+template <typename cx, int M, bool INV>
+__device__ __forceinline__ void columns_fft(cx *Z, int nseq_pad, const cx *tw) {
+    typedef RegFFT<cx, M> RF;
+    constexpr int TT = RF::TT, E1 = RF::E1, S = M + 1;
+    const int t = threadIdx.x % TT, g = threadIdx.x / TT, ng = blockDim.x / TT;
+    for (int base = 0; base < nseq_pad; base += ng) {
+        const int seq = base + g;                  // nseq_pad is a multiple of the groups per warp
+        if (seq < nseq_pad) {
+            cx *col = Z + (size_t)seq * S;
+            cx v[E1];
+#pragma unroll
+            for (int q = 0; q < E1; q++) v[q] = col[RF::in_index(t, q)];
+            __syncwarp();
+            RF::template run<INV>(v, t, col, tw);
+#pragma unroll
+            for (int r = 0; r < RF::R2; r++)
+#pragma unroll
+                for (int k2 = 0; k2 < TT; k2++) col[RF::out_index(t, r, k2)] = v[r * TT + k2];
+        }
+    }
+}
+
+template <typename cx, int M>
+__device__ __forceinline__ void load_cols_nat(cx *dst, const cx *__restrict__ src, const ColSlots &cs, int ns_pad) {
+    constexpr int S = M + 1;
+    for (int e = threadIdx.x; e < ns_pad * M; e += blockDim.x) {
+        const int i = e / ns_pad, sl = e - i * ns_pad;
+        cx v;
+        if (sl < cs.ns) v = src[(size_t)i * M + cs.col[sl]];
+        else { v.x = 0; v.y = 0; }
+        dst[(size_t)sl * S + i] = v;
+    }
+}
+
+template <typename real, int M, int G>
+__global__ void __launch_bounds__(256) kr_boxB(typename Cplx<real>::type *__restrict__ Y1,
+                                               const typename Cplx<real>::type *__restrict__ Y2,
+                                               const unsigned char *__restrict__ clsT, BoxArgs a) {
+    typedef typename Cplx<real>::type cx;
+    constexpr int S = M + 1, WG = BoxGeom<M>::WG;
+    extern __shared__ unsigned char smraw[];
+    cx *tw = (cx *)smraw;
+    fft_twiddles(tw, M);
+    __shared__ ColSlots cs;
+    const int n = blockIdx.y;
+    if (threadIdx.x == 0) make_slots(cs, blockIdx.x * G, G, M);
+    __syncthreads();
+    const int ns_pad = ((cs.ns + WG - 1) / WG) * WG;
+    cx *Z1 = tw + M, *Z2 = Z1 + (size_t)ns_pad * S;
+    load_cols_nat<cx, M>(Z1, Y1 + (size_t)n * M * M, cs, ns_pad);
+    load_cols_nat<cx, M>(Z2, Y2 + (size_t)n * M * M, cs, ns_pad);
+    __syncthreads();
+    columns_fft<cx, M, false>(Z1, 2 * ns_pad, tw);   // Z2 follows Z1 with the same stride
+    __syncthreads();
+    const unsigned char *cl = clsT + (size_t)n * M * M;
+    for_pairs(cs, M, [&](int sa, int ka, int sb, int kb) {
+        const cx z1a = Z1[(size_t)sa * S + ka], z1b = Z1[(size_t)sb * S + kb];
+        const cx z2a = Z2[(size_t)sa * S + ka], z2b = Z2[(size_t)sb * S + kb];
+        cx pxx_a, pyy_a, pxx_b, pyy_b;
+        pxx_a.x = (real)0.5 * (z1a.x + z1b.x); pxx_a.y = (real)0.5 * (z1a.y - z1b.y);
+        pyy_a.x = (real)0.5 * (z1a.y + z1b.y); pyy_a.y = (real)0.5 * (z1b.x - z1a.x);
+        pxx_b.x = pxx_a.x; pxx_b.y = -pxx_a.y;
+        pyy_b.x = pyy_a.x; pyy_b.y = -pyy_a.y;
+        const int ca = cs.col[sa], cb = cs.col[sb];
+        const real kxa = (real)(a.kfac * wrapk(ka, M)), kya = (real)(a.kfac * wrapk(ca, M));
+        const real kxb = (real)(a.kfac * wrapk(kb, M)), kyb = (real)(a.kfac * wrapk(cb, M));
+        const real eta_a = (real)a.visc[cl[(size_t)ca * M + ka]];
+        const real eta_b = (real)a.visc[cl[(size_t)cb * M + kb]];
+        const real fr = (real)a.friction;
+        cx vxa, vya, vxb, vyb;
+        velocity_at<real, cx>(kxa, kya, eta_a, fr, pxx_a, pyy_a, z2a, vxa, vya);
+        velocity_at<real, cx>(kxb, kyb, eta_b, fr, pxx_b, pyy_b, z2b, vxb, vyb);
+        cx hx, hy;
+        hx.x = (real)0.5 * (vxa.x + vxb.x); hx.y = (real)0.5 * (vxa.y - vxb.y);
+        hy.x = (real)0.5 * (vya.x + vyb.x); hy.y = (real)0.5 * (vya.y - vyb.y);
+        cx pa, pb;
+        pa.x = hx.x - hy.y; pa.y = hx.y + hy.x;
+        pb.x = hx.x + hy.y; pb.y = hy.x - hx.y;
+        Z1[(size_t)sa * S + ka] = pa;
+        if (!(sa == sb && ka == kb)) Z1[(size_t)sb * S + kb] = pb;
+    });
+    __syncthreads();
+    columns_fft<cx, M, true>(Z1, ns_pad, tw);
+    __syncthreads();
+    store_cols(Y1 + (size_t)n * M * M, Z1, S, cs, M);
+}
+
+template <typename real, int M, int G>
+__global__ void __launch_bounds__(256) kr_boxD(typename Cplx<real>::type *__restrict__ Y1,
+                                               const typename Cplx<real>::type *__restrict__ Y2, BoxArgs a) {
+    typedef typename Cplx<real>::type cx;
+    constexpr int S = M + 1, WG = BoxGeom<M>::WG;
+    extern __shared__ unsigned char smraw[];
+    cx *tw = (cx *)smraw;
+    fft_twiddles(tw, M);
+    __shared__ ColSlots cs;
+    const int n = blockIdx.y;
+    if (threadIdx.x == 0) make_slots(cs, blockIdx.x * G, G, M);
+    __syncthreads();
+    const int ns_pad = ((cs.ns + WG - 1) / WG) * WG;
+    cx *W = tw + M;
+    load_cols_nat<cx, M>(W, Y2 + (size_t)n * M * M, cs, ns_pad);
+    __syncthreads();
+    columns_fft<cx, M, false>(W, ns_pad, tw);
+    __syncthreads();
+    const real dtk = (real)(a.dt * a.kfac);
+    for_pairs(cs, M, [&](int sa, int ka, int sb, int kb) {
+        const cx wa = W[(size_t)sa * S + ka], wb = W[(size_t)sb * S + kb];
+        cx A1, B1, A2, B2;
+        A1.x = (real)0.5 * (wa.x + wb.x); A1.y = (real)0.5 * (wa.y - wb.y);
+        B1.x = (real)0.5 * (wa.y + wb.y); B1.y = (real)0.5 * (wb.x - wa.x);
+        A2.x = A1.x; A2.y = -A1.y;
+        B2.x = B1.x; B2.y = -B1.y;
+        const real ir1 = (real)wrapk(ka, M), jr1 = (real)wrapk(cs.col[sa], M);
+        const real ir2 = (real)wrapk(kb, M), jr2 = (real)wrapk(cs.col[sb], M);
+        cx F1, F2, D1, D2;
+        F1.x = ir1 * A1.x + jr1 * B1.x; F1.y = ir1 * A1.y + jr1 * B1.y;
+        F2.x = ir2 * A2.x + jr2 * B2.x; F2.y = ir2 * A2.y + jr2 * B2.y;
+        D1.x = dtk * F1.y; D1.y = -dtk * F1.x;
+        D2.x = dtk * F2.y; D2.y = -dtk * F2.x;
+        cx ha, hb;
+        ha.x = (real)0.5 * (D1.x + D2.x); ha.y = (real)0.5 * (D1.y - D2.y);
+        hb.x = ha.x; hb.y = -ha.y;
+        W[(size_t)sa * S + ka] = ha;
+        if (!(sa == sb && ka == kb)) W[(size_t)sb * S + kb] = hb;
+    });
+    __syncthreads();
+    columns_fft<cx, M, true>(W, ns_pad, tw);
+    __syncthreads();
+    store_cols(Y1 + (size_t)n * M * M, W, S, cs, M);
+}
+
 // ---- phi update (cell_phase_functions.cpp:126-217) + normals
 //      (useful_functions.cpp:356-388 with the periodic ghost map of :391-420)
 template <typename real>
@@ -1089,6 +1395,11 @@ struct Fused {
         const BoxArgs ba = box_args(c);
         const int Rr = r->rows_blk, G = r->grp_cols;
         cx *Y1 = (cx *)r->Y1, *Y2 = (cx *)r->Y2;
+        if (M == 256) { PFAG_TRY(box_reg<256>(ba)); }
+        else if (M == 128) { PFAG_TRY(box_reg<128>(ba)); }
+        else if (M == 64) { PFAG_TRY(box_reg<64>(ba)); }
+        else if (M == 32) { PFAG_TRY(box_reg<32>(ba)); }
+        else {
         pfag_prof_begin(c, "kf_boxA");
         kf_boxA<real><<<dim3(M / Rr, Nt), FT, r->smemA, s>>>(R(c->phi), R(c->rho), R(c->lum), R(c->ecm), c->d_xc,
                                                              c->d_yc, ba, Rr, Y1, Y2, R(r->Rb), r->clsT);
@@ -1107,6 +1418,7 @@ struct Fused {
         kf_boxE<real><<<dim3(M / Rr, Nt), FT, r->smemE, s>>>(Y1, R(c->rho), R(r->Rb), R(c->rhon), c->d_xc, c->d_yc,
                                                              ba, Rr);
         PFAG_LAUNCHED(c);
+        }
         // 5. lumen / ECM
         PFAG_CUDA_CHECK(cudaMemsetAsync(r->lK, 0, sizeof(int) * 8, s));
         {
@@ -1161,6 +1473,53 @@ struct Fused {
             kf_rho_ring<real><<<dim3((4 * N + 255) / 256, Nt), 256, 0, s>>>(R(c->rho), N); PFAG_LAUNCHED(c);
         }
         PFAG_CUDA_CHECK(cudaGetLastError());
+        return PFAG_OK;
+    }
+
+    // primaries per block of the column passes (shared tile near 64 KB)
+    static constexpr int GB = sizeof(real) == 8 ? 4 : 8;
+    static constexpr int GD = 2 * GB;
+
+    template <int MM>
+    int box_reg(const BoxArgs &ba) {
+        typedef BoxGeom<MM> BG;
+        cudaStream_t s = c->stream;
+        const int Nt = c->Ntot;
+        const size_t cs = sizeof(cx);
+        const size_t smA = (MM + (size_t)BG::ROWS * MM) * cs + (size_t)BG::ROWS * MM * (sizeof(real) + 1);
+        const size_t smC = (MM + (size_t)BG::ROWS * MM) * cs;
+        const int nsB = ((2 * GB + BG::WG - 1) / BG::WG) * BG::WG, nsD = ((2 * GD + BG::WG - 1) / BG::WG) * BG::WG;
+        const size_t smB = (MM + 2 * (size_t)nsB * (MM + 1)) * cs;
+        const size_t smD = (MM + (size_t)nsD * (MM + 1)) * cs;
+        static bool configured = false;
+        if (!configured) {
+            PFAG_CUDA_CHECK(cudaFuncSetAttribute(kr_boxA<real, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
+            PFAG_CUDA_CHECK(cudaFuncSetAttribute(kr_boxB<real, MM, GB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
+            PFAG_CUDA_CHECK(cudaFuncSetAttribute(kr_boxC<real, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smC));
+            PFAG_CUDA_CHECK(cudaFuncSetAttribute(kr_boxD<real, MM, GD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smD));
+            PFAG_CUDA_CHECK(cudaFuncSetAttribute(kr_boxE<real, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smC));
+            configured = true;
+        }
+        cx *Y1 = (cx *)r->Y1, *Y2 = (cx *)r->Y2;
+        const dim3 grow(MM / BG::ROWS, Nt);
+        pfag_prof_begin(c, "kf_boxA");
+        kr_boxA<real, MM><<<grow, BG::THREADS, smA, s>>>(R(c->phi), R(c->rho), R(c->lum), R(c->ecm), c->d_xc, c->d_yc,
+                                                          ba, Y1, Y2, R(r->Rb), r->clsT);
+        PFAG_LAUNCHED(c);
+        pfag_prof_begin(c, "kf_boxB");
+        kr_boxB<real, MM, GB><<<dim3((MM / 2 + 1 + GB - 1) / GB, Nt), 256, smB, s>>>(Y1, Y2, r->clsT, ba);
+        PFAG_LAUNCHED(c);
+        pfag_prof_begin(c, "kf_boxC");
+        kr_boxC<real, MM><<<grow, BG::THREADS, smC, s>>>(Y1, Y2, R(c->rho), c->d_xc, c->d_yc, ba,
+                                                          c->debug ? R(c->d_vx) : nullptr,
+                                                          c->debug ? R(c->d_vy) : nullptr);
+        PFAG_LAUNCHED(c);
+        pfag_prof_begin(c, "kf_boxD");
+        kr_boxD<real, MM, GD><<<dim3((MM / 2 + 1 + GD - 1) / GD, Nt), 256, smD, s>>>(Y1, Y2, ba);
+        PFAG_LAUNCHED(c);
+        pfag_prof_begin(c, "kf_boxE");
+        kr_boxE<real, MM><<<grow, BG::THREADS, smC, s>>>(Y1, R(c->rho), R(r->Rb), R(c->rhon), c->d_xc, c->d_yc, ba);
+        PFAG_LAUNCHED(c);
         return PFAG_OK;
     }
 
