@@ -32,6 +32,7 @@
 #include <algorithm>
 #include <cmath>
 #include <vector>
+#include <cstdlib>
 
 namespace cg = cooperative_groups;
 
@@ -55,6 +56,8 @@ struct FusedRes {
     int *cK, *cdone, *ccnt; // per cell
     int *lK, *ldone, *lcnt; // [2] lumen, ECM
     int tpc, tiles_i, tiles_j;
+    int resh_threads;       // block size of the reshaping kernel (one thread per zone column)
+    size_t resh_smem;       // its per-warp, per-cell partial sums
     int npsi;
     int coop_r, coop_l;     // co-resident block counts of the persistent kernels
     int logm, rows_blk, grp_cols;
@@ -1032,6 +1035,160 @@ __global__ void kf_reshape(real *__restrict__ phi, real *__restrict__ phin, cons
     }
 }
 
+// Persistent reshaping of all cells (cell_phase_functions.cpp:461-579),
+// register-blocked: a tile is one strip of RI zone rows of one cell, one thread
+// per zone column (blockDim = 32 * ceil(2z/32)); a thread holds its column of
+// the strip plus one halo row each side and takes the left/right neighbours
+// from the adjacent lanes (explicit loads at the warp edges).  Threads past
+// the zone width clamp their loads to the ring column and store nothing.
+// rdev: each warp adds its tiles' sums into its own shared slot per cell (its
+// tiles in a fixed order), the block writes per-cell partials, and after a
+// grid barrier one warp per cell sums the blocks' partials in block order and
+// takes the loop decision; a second barrier publishes it.
+constexpr int RESH_MAX_THREADS = 384;   // 3 warps per SM sub-partition at <= 168 registers
+template <typename real, int RI>
+__global__ void __launch_bounds__(RESH_MAX_THREADS) kf_reshape_strips(real *__restrict__ phi, real *__restrict__ phin, const real *__restrict__ Jc,
+                                  const int *__restrict__ xc, const int *__restrict__ yc, ReshArgs a) {
+    cg::grid_group grid = cg::this_grid();
+    extern __shared__ double wacc[];          // [warps][Ntot]
+    const int N = a.N, z = a.z, Z = 2 * z, W = Z + 2;
+    const real A = (real)a.A, B = (real)a.B;
+    const size_t NN = (size_t)N * N;
+    const int strips = a.tpc;
+    const int total = a.Ntot * strips;
+    const int j = threadIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const bool active_col = j < Z;
+    const int jl = min(j, Z);                 // zone-local column of the loads (Z is the ring)
+    for (int it = 1; it <= a.cap; it++) {
+        real *P = (it & 1) ? phin : phi;
+        real *Q = (it & 1) ? phi : phin;
+        for (int k = threadIdx.x; k < nw * a.Ntot; k += blockDim.x) wacc[k] = 0.0;
+        __syncthreads();
+        for (int t = blockIdx.x; t < total; t += gridDim.x) {
+            const int n = t / strips, strip = t - n * strips;
+            const int d = *(volatile int *)&a.done[n];   // not written during this phase
+            if (d != 0 && d < it) continue;
+            const int zi0 = xc[n] - z, zj0 = yc[n] - z;
+            const int li0 = strip * RI;
+            const int nr = min(RI, Z - li0);
+            const int gj = zj0 + jl;
+            const real *p = P + (size_t)n * NN;
+            const real *Jx = Jc + (size_t)n * 2 * W * W, *Jy = Jx + (size_t)W * W;
+            real pc[RI + 2], pl[RI + 2], pr[RI + 2];
+            real xc_[RI + 2], yc_[RI + 2], xl[RI], xr[RI], yl[RI], yr[RI];
+#pragma unroll
+            for (int r = 0; r < RI + 2; r++) {
+                const int li = min(li0 - 1 + r, Z);           // -1 .. Z (ring rows)
+                pc[r] = p[(size_t)(zi0 + li) * N + gj];
+                const size_t jc = (size_t)(li + 1) * W + (jl + 1);
+                xc_[r] = Jx[jc];
+                yc_[r] = Jy[jc];
+            }
+#pragma unroll
+            for (int r = 0; r < RI + 2; r++) {
+                pl[r] = __shfl_up_sync(0xffffffffu, pc[r], 1);
+                pr[r] = __shfl_down_sync(0xffffffffu, pc[r], 1);
+            }
+#pragma unroll
+            for (int r = 0; r < RI; r++) {
+                xl[r] = __shfl_up_sync(0xffffffffu, xc_[r + 1], 1);
+                xr[r] = __shfl_down_sync(0xffffffffu, xc_[r + 1], 1);
+                yl[r] = __shfl_up_sync(0xffffffffu, yc_[r + 1], 1);
+                yr[r] = __shfl_down_sync(0xffffffffu, yc_[r + 1], 1);
+            }
+            if (lane == 0) {            // left neighbour column jl - 1 >= -1 (ring)
+#pragma unroll
+                for (int r = 0; r < RI + 2; r++) {
+                    const int li = min(li0 - 1 + r, Z);
+                    pl[r] = p[(size_t)(zi0 + li) * N + gj - 1];
+                }
+#pragma unroll
+                for (int r = 0; r < RI; r++) {
+                    const int li = min(li0 + r, Z);
+                    const size_t jc = (size_t)(li + 1) * W + jl;
+                    xl[r] = Jx[jc];
+                    yl[r] = Jy[jc];
+                }
+            }
+            if (lane == 31) {           // right neighbour column min(jl + 1, Z)
+                const int jr = min(jl + 1, Z);
+#pragma unroll
+                for (int r = 0; r < RI + 2; r++) {
+                    const int li = min(li0 - 1 + r, Z);
+                    pr[r] = p[(size_t)(zi0 + li) * N + zj0 + jr];
+                }
+#pragma unroll
+                for (int r = 0; r < RI; r++) {
+                    const int li = min(li0 + r, Z);
+                    const size_t jc = (size_t)(li + 1) * W + jr + 1;
+                    xr[r] = Jx[jc];
+                    yr[r] = Jy[jc];
+                }
+            }
+            double acc = 0.0;
+            real *q = Q + (size_t)n * NN;
+#pragma unroll
+            for (int r = 0; r < RI; r++) {
+                if (r < nr && active_col) {
+                    real w[3][3];
+                    w[0][0] = pl[r];     w[0][1] = pc[r];     w[0][2] = pr[r];
+                    w[1][0] = pl[r + 1]; w[1][1] = pc[r + 1]; w[1][2] = pr[r + 1];
+                    w[2][0] = pl[r + 2]; w[2][1] = pc[r + 2]; w[2][2] = pr[r + 2];
+                    const real old = w[1][1];
+                    const real nv = resh_update<real>(A, B, w, xc_[r + 1], xc_[r + 2], xc_[r], xr[r], xl[r],
+                                                      yc_[r + 1], yc_[r + 2], yc_[r], yr[r], yl[r], old);
+                    q[(size_t)(zi0 + li0 + r) * N + gj] = nv;
+                    acc += fabs((double)nv - (double)old) * a.scale;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) wacc[warp * a.Ntot + n] += acc;
+        }
+        __syncthreads();
+        for (int n = threadIdx.x; n < a.Ntot; n += blockDim.x) {
+            double sum = 0.0;
+            for (int w2 = 0; w2 < nw; w2++) sum += wacc[w2 * a.Ntot + n];
+            a.part[(size_t)n * gridDim.x + blockIdx.x] = sum;
+        }
+        grid.sync();
+        if (warp == 0) {
+            for (int n = blockIdx.x; n < a.Ntot; n += gridDim.x) {
+                const int d = *(volatile int *)&a.done[n];
+                if (d != 0 && d < it) continue;
+                const double rdev = warp_sum_fixed(a.part + (size_t)n * gridDim.x, (int)gridDim.x);
+                if (lane == 0) {
+                    const int done_iters = a.K[n] + 1;
+                    a.K[n] = done_iters;
+                    bool stop = false;
+                    if (done_iters - 1 > a.rimax) { atomicOr(a.err, ERRBIT_RELAX); stop = true; }
+                    if (rdev <= a.thr) stop = true;
+                    if (!stop && it == a.cap) { atomicOr(a.err, ERRBIT_ITER_CAP); stop = true; }
+                    if (stop) a.done[n] = it;
+                }
+            }
+        }
+        grid.sync();
+        bool all = true;
+        for (int n = 0; n < a.Ntot && all; n++) {
+            const int d = *(volatile int *)&a.done[n];
+            all = (d != 0 && d <= it);
+        }
+        if (all) break;
+    }
+    // odd iteration counts leave the last iterate in phi; the reference keeps
+    // the penultimate one there (the copy at the top of its loop), which is in phin
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int n = t / strips, strip = t - n * strips;
+        if (!(a.K[n] & 1) || !active_col) continue;
+        const int zi0 = xc[n] - z, zj0 = yc[n] - z;
+        const int li_end = min(Z, (strip + 1) * RI);
+        for (int li = strip * RI; li < li_end; li++) {
+            const size_t o = (size_t)n * NN + (size_t)(zi0 + li) * N + zj0 + j;
+            phi[o] = phin[o];
+        }
+    }
+}
+
 // ---- persistent lumen / ECM update + reshaping
 //      (cell_phase_functions.cpp:372-444, :709-871; useful_functions.cpp:422-462)
 struct LumArgs {
@@ -1043,7 +1200,6 @@ struct LumArgs {
     double *part;      // [2][gridDim]
     int *K, *done, *cnt;
     unsigned *err;
-    double *sum_ecm_out;
 };
 
 template <typename real>
@@ -1052,67 +1208,81 @@ __device__ __forceinline__ void dirichlet_val(int i, int j, int N, real side, re
     if (edge) v = ((i == 0 || i == N - 1) && (j == 0 || j == N - 1)) ? corner : side;
 }
 
+// sum_ecm = sum h(ECM) dx^2 from the kf_psi block partials, fixed order
+__global__ void kfl_sum_ecm(const double *__restrict__ part, int npart, double *__restrict__ out) {
+    if (threadIdx.x < 32) {
+        const double v = warp_sum_fixed(part, npart);
+        if (threadIdx.x == 0) *out = v;
+    }
+}
+
+// update_lumen_and_ECM (cell_phase_functions.cpp:372-444) with the boundary
+// values of boundary_conditions_lumen_and_ECM (useful_functions.cpp:439-462)
+template <typename real>
+__global__ void kfl_update(const real *__restrict__ lum, const real *__restrict__ ecm, real *__restrict__ lumn,
+                           real *__restrict__ ecmn, const real *__restrict__ psi, const real *__restrict__ hl,
+                           const real *__restrict__ he, const double *__restrict__ sum_ecm, LumArgs a) {
+    const int N = a.N;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N || j >= N) return;
+    const size_t k = (size_t)i * N + j;
+    if (i == 0 || i == N - 1 || j == 0 || j == N - 1) { lumn[k] = (real)0.0; ecmn[k] = (real)1.0; return; }
+    const real dx = (real)a.dx, dt = (real)a.dt, q4 = (real)4.0 * dx * dx;
+    const real elastic = (real)(a.alpha_ECM * ((double)N * (double)N * a.dx * a.dx - *sum_ecm));
+    const real sv = psi[k];
+    const real L = lap9<real>(sv, psi[k + N], psi[k - N], psi[k + 1], psi[k - 1], psi[k + N + 1], psi[k + N - 1],
+                              psi[k - N - 1], psi[k - N + 1]);
+    const real l = lum[k], e = ecm[k];
+    real ln = l;
+    ln += ((real)1.0 / (real)a.tau_lum) * l * ((real)1.0 - l) * dt *
+          ((real)a.xi_lum - (real)a.beta_lum_cells * sv + (real)a.eta_lum_cells * L / q4 - (real)a.beta_lum_ECM * he[k]);
+    real en = e;
+    en += ((real)1.0 / (real)a.tau_ECM) * e * ((real)1.0 - e) * dt *
+          (elastic + (real)a.xi_ECM - (real)a.beta_ECM_cells * sv + (real)a.eta_ECM_cells * L / q4 -
+           (real)a.beta_lum_ECM * hl[k]);
+    lumn[k] = ln;
+    ecmn[k] = en;
+}
+
+// normals J = (1/(2dx)) grad(field_new) / |grad field_old| on every site, ghost
+// sites through the periodic map (cell_phase_functions.cpp:722-771)
+template <typename real>
+__global__ void kfl_normals(const real *__restrict__ lum, const real *__restrict__ lumn, const real *__restrict__ ecm,
+                            const real *__restrict__ ecmn, real *__restrict__ Jl, int N, double dx) {
+    const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N || j >= N) return;
+    const size_t NN = (size_t)N * N, k = (size_t)i * N + j;
+    const size_t c = (size_t)ghost_src(i, N) * N + ghost_src(j, N);
+    const real c4 = (real)(1.0 / dx / dx / 4.0), inv2dx = (real)(1.0 / (2.0 * dx));
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+        const real *o = f ? ecm : lum;
+        const real *nw = f ? ecmn : lumn;
+        const real ga = o[c + N] - o[c - N], gb = o[c + 1] - o[c - 1];
+        const real g = sqrt(c4 * (ga * ga + gb * gb));
+        Jl[(size_t)(2 * f) * NN + k] = (g != (real)0.0) ? inv2dx * (nw[c + N] - nw[c - N]) / g : (real)0.0;
+        Jl[(size_t)(2 * f + 1) * NN + k] = (g != (real)0.0) ? inv2dx * (nw[c + 1] - nw[c - 1]) / g : (real)0.0;
+    }
+}
+
+// Persistent relaxation of the lumen and ECM fields (cell_phase_functions.cpp:774-869)
 template <typename real>
 __global__ void kf_lum(real *__restrict__ lum, real *__restrict__ lumn, real *__restrict__ ecm,
-                       real *__restrict__ ecmn, const real *__restrict__ psi, const real *__restrict__ hl,
-                       const real *__restrict__ he, real *__restrict__ Jl, LumArgs a) {
+                       real *__restrict__ ecmn, const real *__restrict__ Jl, LumArgs a) {
     cg::grid_group grid = cg::this_grid();
     const int N = a.N;
     const size_t NN = (size_t)N * N;
-    __shared__ double s_sum;
     __shared__ int s_last, s_skip;
-    // sum_ecm in a fixed order (every block computes the same value)
-    if (threadIdx.x == 0) {
-        double sacc = 0.0;
-        for (int b = 0; b < a.npsi; b++) sacc += a.part_e[b];
-        s_sum = sacc;
-        if (blockIdx.x == 0) *a.sum_ecm_out = sacc;
-    }
-    __syncthreads();
-    const double sum_ecm = s_sum;
-    const real dx = (real)a.dx, dt = (real)a.dt, q4 = (real)4.0 * dx * dx;
-    const real elastic = (real)(a.alpha_ECM * ((double)N * (double)N * a.dx * a.dx - sum_ecm));
-    // phase U: lumn / ECMn (interior), Dirichlet sides (lumen 0, ECM 1, corners as their sides)
-    for (int i = blockIdx.x; i < N; i += gridDim.x)
-      for (int j = threadIdx.x; j < N; j += blockDim.x) {
-        const size_t k = (size_t)i * N + j;
-        if (i == 0 || i == N - 1 || j == 0 || j == N - 1) { lumn[k] = (real)0.0; ecmn[k] = (real)1.0; continue; }
-        const real s = psi[k];
-        const real L = lap9<real>(s, psi[k + N], psi[k - N], psi[k + 1], psi[k - 1], psi[k + N + 1], psi[k + N - 1],
-                                  psi[k - N - 1], psi[k - N + 1]);
-        const real l = lum[k], e = ecm[k];
-        real ln = l;
-        ln += ((real)1.0 / (real)a.tau_lum) * l * ((real)1.0 - l) * dt *
-              ((real)a.xi_lum - (real)a.beta_lum_cells * s + (real)a.eta_lum_cells * L / q4 -
-               (real)a.beta_lum_ECM * he[k]);
-        real en = e;
-        en += ((real)1.0 / (real)a.tau_ECM) * e * ((real)1.0 - e) * dt *
-              (elastic + (real)a.xi_ECM - (real)a.beta_ECM_cells * s + (real)a.eta_ECM_cells * L / q4 -
-               (real)a.beta_lum_ECM * hl[k]);
-        lumn[k] = ln;
-        ecmn[k] = en;
-    }
-    grid.sync();
-    // phase N: normals J = (1/(2dx)) grad(field_new) / |grad field_old| on every
-    // site, ghost sites through the periodic map (cell_phase_functions.cpp:722-771)
-    const real c4 = (real)(1.0 / a.dx / a.dx / 4.0), inv2dx = (real)(1.0 / (2.0 * a.dx));
-    for (int i = blockIdx.x; i < N; i += gridDim.x)
-      for (int j = threadIdx.x; j < N; j += blockDim.x) {
-        const size_t k = (size_t)i * N + j;
-        const size_t c = (size_t)ghost_src(i, N) * N + ghost_src(j, N);
-        for (int f = 0; f < 2; f++) {
-            const real *o = f ? ecm : lum;
-            const real *nw = f ? ecmn : lumn;
-            const real ga = o[c + N] - o[c - N], gb = o[c + 1] - o[c - 1];
-            const real g = sqrt(c4 * (ga * ga + gb * gb));
-            Jl[(size_t)(2 * f) * NN + k] = (g != (real)0.0) ? inv2dx * (nw[c + N] - nw[c - N]) / g : (real)0.0;
-            Jl[(size_t)(2 * f + 1) * NN + k] = (g != (real)0.0) ? inv2dx * (nw[c + 1] - nw[c - 1]) / g : (real)0.0;
-        }
-    }
-    grid.sync();
-    // phase R: relaxation loops of both fields, iteration k reads P, writes Q
+    // phase R: relaxation loops of both fields, iteration k reads P, writes Q.
+    // Tiles of LRI rows x blockDim columns; one thread per column with its
+    // column of the strip (plus a halo row each side) in registers and the
+    // left/right neighbours from the adjacent lanes.
     const real A = (real)a.A, B = (real)a.B;
     const double dx2 = a.dx * a.dx;
+    constexpr int LRI = 4;
+    const int lane = threadIdx.x & 31;
+    const int tiles_i = (N + LRI - 1) / LRI, tiles_j = (N + blockDim.x - 1) / blockDim.x;
+    const int ntiles = tiles_i * tiles_j;
     for (int it = 1; it <= a.cap; it++) {
         for (int f = 0; f < 2; f++) {
             if (threadIdx.x == 0) {
@@ -1128,21 +1298,68 @@ __global__ void kf_lum(real *__restrict__ lum, real *__restrict__ lumn, real *__
             const real side = f ? (real)1.0 : (real)0.0;
             const real *Jx = Jl + (size_t)(2 * f) * NN, *Jy = Jl + (size_t)(2 * f + 1) * NN;
             double acc = 0.0;
-            for (int i = blockIdx.x; i < N; i += gridDim.x)
-              for (int j = threadIdx.x; j < N; j += blockDim.x) {
-                const size_t k = (size_t)i * N + j;
-                real v;
-                bool edge;
-                dirichlet_val<real>(i, j, N, side, (real)0.0, v, edge);
-                if (!edge) {
-                    real w[3][3];
-                    for (int u = 0; u < 3; u++)
-                        for (int q = 0; q < 3; q++) w[u][q] = P[k + (size_t)(u - 1) * N + (q - 1)];
-                    v = resh_update<real>(A, B, w, Jx[k], Jx[k + N], Jx[k - N], Jx[k + 1], Jx[k - 1], Jy[k],
-                                          Jy[k + N], Jy[k - N], Jy[k + 1], Jy[k - 1], w[1][1]);
+            for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+                const int ti = tile / tiles_j, tj = tile - ti * tiles_j;
+                const int i0 = ti * LRI;
+                const int jraw = tj * blockDim.x + threadIdx.x;
+                const bool col_ok = jraw < N;
+                const int jj = min(jraw, N - 1);
+                real pc[LRI + 2], pl[LRI + 2], pr[LRI + 2], xc_[LRI + 2], yc_[LRI + 2];
+                real xl[LRI], xr[LRI], yl[LRI], yr[LRI];
+#pragma unroll
+                for (int r = 0; r < LRI + 2; r++) {
+                    const int ii = min(max(i0 - 1 + r, 0), N - 1);
+                    const size_t k = (size_t)ii * N + jj;
+                    pc[r] = P[k];
+                    xc_[r] = Jx[k];
+                    yc_[r] = Jy[k];
                 }
-                acc += fabs((double)v - (double)P[k]) * dx2;
-                Q[k] = v;
+#pragma unroll
+                for (int r = 0; r < LRI + 2; r++) {
+                    pl[r] = __shfl_up_sync(0xffffffffu, pc[r], 1);
+                    pr[r] = __shfl_down_sync(0xffffffffu, pc[r], 1);
+                }
+#pragma unroll
+                for (int r = 0; r < LRI; r++) {
+                    xl[r] = __shfl_up_sync(0xffffffffu, xc_[r + 1], 1);
+                    xr[r] = __shfl_down_sync(0xffffffffu, xc_[r + 1], 1);
+                    yl[r] = __shfl_up_sync(0xffffffffu, yc_[r + 1], 1);
+                    yr[r] = __shfl_down_sync(0xffffffffu, yc_[r + 1], 1);
+                }
+                if (lane == 0 || lane == 31) {
+                    const int jn = lane == 0 ? max(jj - 1, 0) : min(jj + 1, N - 1);
+#pragma unroll
+                    for (int r = 0; r < LRI + 2; r++) {
+                        const int ii = min(max(i0 - 1 + r, 0), N - 1);
+                        const real v = P[(size_t)ii * N + jn];
+                        if (lane == 0) pl[r] = v; else pr[r] = v;
+                    }
+#pragma unroll
+                    for (int r = 0; r < LRI; r++) {
+                        const int ii = min(i0 + r, N - 1);
+                        const size_t k = (size_t)ii * N + jn;
+                        if (lane == 0) { xl[r] = Jx[k]; yl[r] = Jy[k]; } else { xr[r] = Jx[k]; yr[r] = Jy[k]; }
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < LRI; r++) {
+                    const int ii = i0 + r;
+                    if (ii < N && col_ok) {
+                        real v;
+                        bool edge;
+                        dirichlet_val<real>(ii, jj, N, side, (real)0.0, v, edge);
+                        if (!edge) {
+                            real w[3][3];
+                            w[0][0] = pl[r];     w[0][1] = pc[r];     w[0][2] = pr[r];
+                            w[1][0] = pl[r + 1]; w[1][1] = pc[r + 1]; w[1][2] = pr[r + 1];
+                            w[2][0] = pl[r + 2]; w[2][1] = pc[r + 2]; w[2][2] = pr[r + 2];
+                            v = resh_update<real>(A, B, w, xc_[r + 1], xc_[r + 2], xc_[r], xr[r], xl[r], yc_[r + 1],
+                                                  yc_[r + 2], yc_[r], yr[r], yl[r], w[1][1]);
+                        }
+                        acc += fabs((double)v - (double)pc[r + 1]) * dx2;
+                        Q[(size_t)ii * N + jj] = v;
+                    }
+                }
             }
             const double bs = block_sum_d(acc);
             if (threadIdx.x == 0) {
@@ -1243,21 +1460,36 @@ BoxArgs box_args(pfag_ctx *c) {
     return a;
 }
 
-template <typename real>
-int launch_coop(const void *fn, int blocks, void **args, size_t smem, cudaStream_t s) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(blocks);
-    cfg.blockDim = dim3(FT);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    PFAG_CUDA_CHECK(cudaLaunchKernelExC(&cfg, fn, args));
-    return PFAG_OK;
+// Cooperative launch; when the runtime refuses the grid as larger than what
+// can be co-resident, the grid is halved (the kernels stride over their work)
+// and *blocks keeps the accepted size for later launches.
+inline int launch_coop_t(const void *fn, int *blocks, int threads, void **args, size_t smem, cudaStream_t s) {
+    for (;;) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(*blocks);
+        cfg.blockDim = dim3(threads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
+        if (e == cudaSuccess) return PFAG_OK;
+        if (e == cudaErrorCooperativeLaunchTooLarge && *blocks > 1) {
+            (void)cudaGetLastError();
+            *blocks /= 2;
+            continue;
+        }
+        cudaFuncAttributes fa{};
+        cudaFuncGetAttributes(&fa, fn);
+        pfag_set_error("cooperative launch of %d x %d threads (%d registers/thread, %zu B static smem): %s", *blocks,
+                       threads, fa.numRegs, fa.sharedSizeBytes, cudaGetErrorString(e));
+        return PFAG_E_CUDA;
+    }
 }
+
 
 template <typename real>
 struct Fused {
@@ -1298,11 +1530,23 @@ struct Fused {
         int dev = 0, nsm = 0, per = 0;
         PFAG_CUDA_CHECK(cudaGetDevice(&dev));
         PFAG_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kf_reshape<real>, FT, 0));
-        r->coop_r = std::max(1, nsm * std::min(per, 4));
+        r->resh_threads = 32 * ((2 * c->zone + 31) / 32);
+        if (r->resh_threads > RESH_MAX_THREADS) {
+            pfag_set_error("fused path: zone width 2*%d above %d columns; use the plain path", c->zone, RESH_MAX_THREADS);
+            return PFAG_E_UNSUPPORTED;
+        }
+        r->resh_smem = (size_t)(r->resh_threads / 32) * c->Ntot * sizeof(double);
+        if (r->resh_smem > 200 * 1024) { pfag_set_error("too many cells for the reshaping kernel's per-warp sums"); return PFAG_E_UNSUPPORTED; }
+        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_reshape_strips<real, RESH_RI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)r->resh_smem));
+        PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kf_reshape_strips<real, RESH_RI>,
+                                                                       r->resh_threads, r->resh_smem));
+        if (per < 1) { pfag_set_error("reshaping kernel cannot be resident with %d threads", r->resh_threads); return PFAG_E_UNSUPPORTED; }
+        r->coop_r = nsm * std::min(per, 8);
         PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kf_lum<real>, FT, 0));
-        r->coop_l = std::max(1, nsm * std::min(per, 4));
-        r->tiles_i = (2 * c->zone + RT_I - 1) / RT_I;
+        if (per < 1) { pfag_set_error("lumen/ECM kernel cannot be resident"); return PFAG_E_UNSUPPORTED; }
+        r->coop_l = nsm * std::min(per, 4);
+        r->tiles_i = (2 * c->zone + RESH_RI - 1) / RESH_RI;
         r->tiles_j = 1;
         r->tpc = r->tiles_i;
         r->npsi = ((c->N + 31) / 32) * ((c->N + 31) / 32);
@@ -1320,7 +1564,7 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaMalloc(&r->Jl, 4 * c->ng * rs));
         PFAG_CUDA_CHECK(cudaMalloc(&r->rect, sizeof(int4) * c->Ntot));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_s, sizeof(double) * c->Ntot * SBLK));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->part_r, sizeof(double) * (size_t)c->Ntot * r->tpc));
+        PFAG_CUDA_CHECK(cudaMalloc(&r->part_r, sizeof(double) * (size_t)c->Ntot * std::max(r->tpc, r->coop_r)));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_e, sizeof(double) * r->npsi));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_l, sizeof(double) * 2 * r->coop_l));
         PFAG_CUDA_CHECK(cudaMalloc(&r->cK, sizeof(int) * (3 * c->Ntot + 8)));
@@ -1430,14 +1674,23 @@ struct Fused {
             la.beta_ECM_cells = d.beta_ECM_cells; la.eta_ECM_cells = d.eta_ECM_cells;
             la.A = d.A_resh; la.B = d.B_resh; la.thr = d.thr_lum; la.rdev0 = d.rdev0_lum;
             la.part_e = r->part_e; la.part = r->part_l; la.K = r->lK; la.done = r->ldone; la.cnt = r->lcnt;
-            la.err = c->d_err; la.sum_ecm_out = c->d_scal + 0;
-            real *a0 = R(c->lum), *a1 = R(c->lumn), *a2 = R(c->ecm), *a3 = R(c->ecmn), *a5 = R(c->hlum),
-                 *a6 = R(c->hecm), *a7 = R(r->Jl);
-            const real *a4 = R(c->psi);
-            const real *a5c = a5, *a6c = a6;
-            void *args[] = {&a0, &a1, &a2, &a3, (void *)&a4, (void *)&a5c, (void *)&a6c, &a7, &la};
+            la.err = c->d_err;
+            pfag_prof_begin(c, "kfl_sum_ecm");
+            kfl_sum_ecm<<<1, 32, 0, s>>>(r->part_e, r->npsi, c->d_scal + 0);
+            PFAG_LAUNCHED(c);
+            const dim3 tb(32, 8), gb((N + 31) / 32, (N + 7) / 8);
+            pfag_prof_begin(c, "kfl_update");
+            kfl_update<real><<<gb, tb, 0, s>>>(R(c->lum), R(c->ecm), R(c->lumn), R(c->ecmn), R(c->psi), R(c->hlum),
+                                               R(c->hecm), c->d_scal + 0, la);
+            PFAG_LAUNCHED(c);
+            pfag_prof_begin(c, "kfl_normals");
+            kfl_normals<real><<<gb, tb, 0, s>>>(R(c->lum), R(c->lumn), R(c->ecm), R(c->ecmn), R(r->Jl), N, d.dx);
+            PFAG_LAUNCHED(c);
+            real *a0 = R(c->lum), *a1 = R(c->lumn), *a2 = R(c->ecm), *a3 = R(c->ecmn);
+            const real *a4 = R(r->Jl);
+            void *args[] = {&a0, &a1, &a2, &a3, (void *)&a4, &la};
             pfag_prof_begin(c, "kf_lum");
-            PFAG_TRY(launch_coop<real>((const void *)kf_lum<real>, r->coop_l, args, 0, s));
+            PFAG_TRY(launch_coop_t((const void *)kf_lum<real>, &r->coop_l, FT, args, 0, s));
             PFAG_LAUNCHED(c);
         }
         // 6. phi update + normals, then reshaping
@@ -1461,7 +1714,8 @@ struct Fused {
             const int *a3 = c->d_xc, *a4 = c->d_yc;
             void *args[] = {&a0, &a1, (void *)&a2, (void *)&a3, (void *)&a4, &ra};
             pfag_prof_begin(c, "kf_reshape");
-            PFAG_TRY(launch_coop<real>((const void *)kf_reshape<real>, r->coop_r, args, 0, s));
+            PFAG_TRY(launch_coop_t((const void *)kf_reshape_strips<real, RESH_RI>, &r->coop_r, r->resh_threads, args,
+                                   r->resh_smem, s));
             PFAG_LAUNCHED(c);
         }
         // 7. rho <- rhon on the boxes, ghost ring
@@ -1475,6 +1729,9 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaGetLastError());
         return PFAG_OK;
     }
+
+    // rows per reshaping strip (registers: ~10 reals per row and thread)
+    static constexpr int RESH_RI = 4;
 
     // primaries per block of the column passes (shared tile near 64 KB)
     static constexpr int GB = sizeof(real) == 8 ? 4 : 8;
@@ -1525,6 +1782,13 @@ struct Fused {
 
     int stats() {
         const int Nt = c->Ntot;
+        if (std::getenv("PFAG_DEBUG_COOP")) {
+            cudaFuncAttributes fr{}, fl{};
+            cudaFuncGetAttributes(&fr, (const void *)kf_reshape_strips<real, RESH_RI>);
+            cudaFuncGetAttributes(&fl, (const void *)kf_lum<real>);
+            std::fprintf(stderr, "pfag coop: reshape %d blocks x %d threads (%d regs), lum %d blocks x %d (%d regs)\n",
+                         r->coop_r, r->resh_threads, fr.numRegs, r->coop_l, FT, fl.numRegs);
+        }
         std::vector<int> h(3 * Nt + 8);
         PFAG_CUDA_CHECK(cudaMemcpyAsync(h.data(), r->cK, sizeof(int) * (3 * Nt + 8), cudaMemcpyDeviceToHost, c->stream));
         PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
