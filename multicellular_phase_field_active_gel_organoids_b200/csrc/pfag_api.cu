@@ -57,6 +57,10 @@ static DevParams make_devparams(const pfag_params &p) {
     d.rdev0_lum = (double)(2 * p.rdev_threshold) * p.rtol * p.rdt;  // :720 (rdev_ini = 2*rdev_threshold)
     d.kfac = 2.0 * M_PI / ((2 * p.zone_size - 2) * p.dx);           // rho_functions.cpp:164
     d.inv_norm = 1.0 / ((double)d.M * (double)d.M);
+    d.k_cpl = p.coupling_PF_AG / p.tau * (p.dt / p.dx / p.dx / 4.0) / std::sqrt(2.0 * M_PI) / p.sigma;
+    d.inv_2s2 = 1.0 / (2.0 * p.sigma * p.sigma);
+    d.dt_tau = p.dt / p.tau;
+    d.inv_q4 = 1.0 / (4.0 * p.dx * p.dx);
     // rho_functions.cpp:355-397: 0 apical, 1 basal, 2 lateral
     d.deg[0] = p.degrate_apical; d.deg[1] = p.degrate_basal; d.deg[2] = p.degrate_lateral;
     d.gen[0] = p.matgenrate_apical; d.gen[1] = p.matgenrate_basal; d.gen[2] = p.matgenrate_lateral;

@@ -201,29 +201,34 @@ template <typename real>
 __global__ void kf_psi(const real *__restrict__ hfunc, const int4 *__restrict__ rect, int Ntot, int N,
                        const real *__restrict__ lum, const real *__restrict__ ecm, real *__restrict__ psi,
                        real *__restrict__ hl, real *__restrict__ he, double dx2, double *__restrict__ part) {
+    // cells whose support rectangle meets this 32x32 tile, in ascending order
+    // (the reference sums n = 0 .. Ntot-1): warp 0 compacts them by ballots
     __shared__ int list[1024];
+    __shared__ int4 lrect[1024];
     __shared__ int nlist;
     const int ti0 = blockIdx.y * 32, tj0 = blockIdx.x * 32;
-    if (threadIdx.x == 0) nlist = 0;
-    __syncthreads();
-    for (int n = threadIdx.x; n < Ntot; n += blockDim.x) {
-        int4 r = rect[n];
-        if (r.x < ti0 + 32 && r.y > ti0 && r.z < tj0 + 32 && r.w > tj0) {
-            int slot = atomicAdd(&nlist, 1);
-            if (slot < 1024) list[slot] = n;
+    if (threadIdx.x < 32) {
+        int cnt = 0;
+        for (int base = 0; base < Ntot; base += 32) {
+            const int n = base + threadIdx.x;
+            int4 r = make_int4(0, 0, 0, 0);
+            bool hit = false;
+            if (n < Ntot) {
+                r = rect[n];
+                hit = r.x < ti0 + 32 && r.y > ti0 && r.z < tj0 + 32 && r.w > tj0;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (hit) {
+                const int slot = cnt + __popc(m & ((1u << threadIdx.x) - 1u));
+                list[slot] = n;
+                lrect[slot] = r;
+            }
+            cnt += __popc(m);
         }
+        if (threadIdx.x == 0) nlist = cnt;
     }
     __syncthreads();
-    const int nl = min(nlist, 1024);
-    // ascending cell order (the reference sums n = 0 .. Ntot-1)
-    if (threadIdx.x == 0) {
-        for (int a = 1; a < nl; a++) {
-            int v = list[a], b = a - 1;
-            while (b >= 0 && list[b] > v) { list[b + 1] = list[b]; b--; }
-            list[b + 1] = v;
-        }
-    }
-    __syncthreads();
+    const int nl = nlist;
     double acc = 0.0;
     for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
         const int i = ti0 + (e >> 5), j = tj0 + (e & 31);
@@ -231,9 +236,8 @@ __global__ void kf_psi(const real *__restrict__ hfunc, const int4 *__restrict__ 
         const size_t s = (size_t)i * N + j;
         real sum = (real)0.0;
         for (int q = 0; q < nl; q++) {
-            const int n = list[q];
-            const int4 r = rect[n];
-            if (i >= r.x && i < r.y && j >= r.z && j < r.w) sum += hfunc[(size_t)n * N * N + s];
+            const int4 r = lrect[q];
+            if (i >= r.x && i < r.y && j >= r.z && j < r.w) sum += hfunc[(size_t)list[q] * N * N + s];
         }
         psi[s] = sum;
         const real a = lum[s], b = ecm[s];
@@ -250,6 +254,7 @@ __global__ void kf_psi(const real *__restrict__ hfunc, const int4 *__restrict__ 
 struct BoxArgs {
     int N, z, M, logm, Ntot;
     double c4, sigma, dt, kfac, friction, dx;
+    double inv_2s2, k_delta;     // 1/(2 sigma^2), 1/(sqrt(2 pi) sigma): FP32 folded constants
     double deg[3], gen[3], a_ort[3], a_tan[3], visc[3], bb[3];
 };
 
@@ -325,6 +330,14 @@ __device__ __forceinline__ void velocity_at(real kx, real ky, real et, real fric
     const real D = -((real)4.0 * et * et * kx * kx * ky * ky + friction * friction +
                      (real)3.0 * et * friction * (kx * kx + ky * ky) +
                      (real)2.0 * et * et * (kx * kx * kx * kx + ky * ky * ky * ky));
+    if constexpr (sizeof(real) == 4) {
+        const real iD = (real)1.0 / D, iA = (real)1.0 / A;
+        vy.x = (et * kx * ky * (kx * pxx.y + ky * pxy.y) - A * (ky * pyy.y + kx * pxy.y)) * iD;
+        vy.y = (-et * kx * ky * (kx * pxx.x + ky * pxy.x) + A * (ky * pyy.x + kx * pxy.x)) * iD;
+        vx.x = (kx * pxx.y + ky * pxy.y - et * kx * ky * vy.x) * iA;
+        vx.y = (-kx * pxx.x - ky * pxy.x - et * kx * ky * vy.y) * iA;
+        return;
+    }
     vy.x = (real)0.0 + et * kx * ky * (kx * pxx.y + ky * pxy.y);
     vy.x -= A * (ky * pyy.y + kx * pxy.y);
     vy.x /= D;
@@ -596,7 +609,7 @@ __global__ void __launch_bounds__(256) kr_boxA(const real *__restrict__ phi, con
     cx *tw = (cx *)smraw;
     cx *scr = tw + M;                                   // [ROWS][M] exchange scratch
     real *xys = (real *)(scr + ROWS * M);               // [ROWS][M] pi_xy, read back by the same thread
-    unsigned char *cls = (unsigned char *)(xys + ROWS * M);  // [ROWS][M]
+    unsigned char *cls = (unsigned char *)(xys + ROWS * M);  // [ROWS][M + 4]: padded against bank conflicts
     fft_twiddles(tw, M);
     __syncthreads();
     const int t = threadIdx.x % TT, g = threadIdx.x / TT;
@@ -623,15 +636,27 @@ __global__ void __launch_bounds__(256) kr_boxA(const real *__restrict__ phi, con
         const real at = (real)a.a_tan[c], ao = (real)a.a_ort[c], b = (real)a.bb[c];
         real xx = -at * rr * rr * rr + b * rr * rr * rr * rr;
         real yy = xx, xy = (real)0.0;
-        if (gg > (real)0.0) {
-            xx += (at - ao) * rr * rr * rr * c4 * dxp * dxp / gg / gg;
-            yy += (at - ao) * rr * rr * rr * c4 * dyp * dyp / gg / gg;
-            xy += (at - ao) * rr * rr * rr * c4 * dxp * dyp / gg / gg;
+        real P;
+        if constexpr (sizeof(real) == 8) {
+            if (gg > (real)0.0) {
+                xx += (at - ao) * rr * rr * rr * c4 * dxp * dxp / gg / gg;
+                yy += (at - ao) * rr * rr * rr * c4 * dyp * dyp / gg / gg;
+                xy += (at - ao) * rr * rr * rr * c4 * dxp * dyp / gg / gg;
+            }
+            P = gg * exp(-(f - (real)0.5) * (f - (real)0.5) / (real)2.0 / sigma / sigma) / sqrt((real)(2.0 * M_PI)) /
+                sigma;
+        } else {
+            if (gg > (real)0.0) {
+                const real w = (at - ao) * rr * rr * rr * c4 / (gg * gg);
+                xx += w * dxp * dxp;
+                yy += w * dyp * dyp;
+                xy += w * dxp * dyp;
+            }
+            const real d = f - (real)0.5;
+            P = gg * (real)a.k_delta * __expf(-d * d * (real)a.inv_2s2);
         }
-        const real P = gg * exp(-(f - (real)0.5) * (f - (real)0.5) / (real)2.0 / sigma / sigma) /
-                       sqrt((real)(2.0 * M_PI)) / sigma;
         Rb[rowo + j] = -(real)a.deg[c] * rr + (real)a.gen[c] * P;
-        cls[g * M + j] = (unsigned char)c;
+        cls[g * (M + 4) + j] = (unsigned char)c;
         xys[g * M + j] = xy;
         v[q].x = xx;
         v[q].y = yy;
@@ -655,7 +680,7 @@ __global__ void __launch_bounds__(256) kr_boxA(const real *__restrict__ phi, con
     // class map transposed, ROWS consecutive bytes per column
     for (int e = threadIdx.x; e < M * ROWS; e += blockDim.x) {
         const int j = e / ROWS, r = e % ROWS;
-        clsT[((size_t)n * M + j) * M + i0 + r] = cls[r * M + j];
+        clsT[((size_t)n * M + j) * M + i0 + r] = cls[r * (M + 4) + j];
     }
 }
 
@@ -768,16 +793,34 @@ __device__ __forceinline__ void columns_fft(cx *Z, int nseq_pad, const cx *tw) {
     }
 }
 
-template <typename cx, int M>
-__device__ __forceinline__ void load_cols_nat(cx *dst, const cx *__restrict__ src, const ColSlots &cs, int ns_pad) {
-    constexpr int S = M + 1;
-    for (int e = threadIdx.x; e < ns_pad * M; e += blockDim.x) {
-        const int i = e / ns_pad, sl = e - i * ns_pad;
+// Column strips: NSP (a power of two) slots of M complex each, stride M + 1.
+// Thread t always handles slot t % NSP and rows t / NSP + k * (blockDim / NSP),
+// so the loop has shift-only indexing and independent loads; slots past the
+// block's columns are zero and never stored.
+template <typename cx, int M, int NSP>
+__device__ __forceinline__ void load_cols_fixed(cx *dst, const cx *__restrict__ src, const ColSlots &cs) {
+    constexpr int S = M + 1, STEP = 256 / NSP;
+    static_assert(NSP <= 256 && (NSP & (NSP - 1)) == 0, "NSP must be a power of two <= 256");
+    const int sl = threadIdx.x % NSP, i0 = threadIdx.x / NSP;
+    const bool live = sl < cs.ns;
+    const int col = live ? cs.col[sl] : 0;
+#pragma unroll 8
+    for (int i = i0; i < M; i += STEP) {
         cx v;
-        if (sl < cs.ns) v = src[(size_t)i * M + cs.col[sl]];
+        if (live) v = src[(size_t)i * M + col];
         else { v.x = 0; v.y = 0; }
         dst[(size_t)sl * S + i] = v;
     }
+}
+
+template <typename cx, int M, int NSP>
+__device__ __forceinline__ void store_cols_fixed(cx *__restrict__ dstg, const cx *src, const ColSlots &cs) {
+    constexpr int S = M + 1, STEP = 256 / NSP;
+    const int sl = threadIdx.x % NSP, i0 = threadIdx.x / NSP;
+    if (sl >= cs.ns) return;
+    const int col = cs.col[sl];
+#pragma unroll 8
+    for (int i = i0; i < M; i += STEP) dstg[(size_t)i * M + col] = src[(size_t)sl * S + i];
 }
 
 template <typename real, int M, int G>
@@ -793,12 +836,13 @@ __global__ void __launch_bounds__(256) kr_boxB(typename Cplx<real>::type *__rest
     const int n = blockIdx.y;
     if (threadIdx.x == 0) make_slots(cs, blockIdx.x * G, G, M);
     __syncthreads();
-    const int ns_pad = ((cs.ns + WG - 1) / WG) * WG;
-    cx *Z1 = tw + M, *Z2 = Z1 + (size_t)ns_pad * S;
-    load_cols_nat<cx, M>(Z1, Y1 + (size_t)n * M * M, cs, ns_pad);
-    load_cols_nat<cx, M>(Z2, Y2 + (size_t)n * M * M, cs, ns_pad);
+    constexpr int NSP = 2 * G;               // slots per block (primaries and partners, padded)
+    static_assert(NSP % WG == 0, "slot count must be a multiple of the thread groups per warp");
+    cx *Z1 = tw + M, *Z2 = Z1 + (size_t)NSP * S;
+    load_cols_fixed<cx, M, NSP>(Z1, Y1 + (size_t)n * M * M, cs);
+    load_cols_fixed<cx, M, NSP>(Z2, Y2 + (size_t)n * M * M, cs);
     __syncthreads();
-    columns_fft<cx, M, false>(Z1, 2 * ns_pad, tw);   // Z2 follows Z1 with the same stride
+    columns_fft<cx, M, false>(Z1, 2 * NSP, tw);   // Z2 follows Z1 with the same stride
     __syncthreads();
     const unsigned char *cl = clsT + (size_t)n * M * M;
     for_pairs(cs, M, [&](int sa, int ka, int sb, int kb) {
@@ -828,9 +872,9 @@ __global__ void __launch_bounds__(256) kr_boxB(typename Cplx<real>::type *__rest
         if (!(sa == sb && ka == kb)) Z1[(size_t)sb * S + kb] = pb;
     });
     __syncthreads();
-    columns_fft<cx, M, true>(Z1, ns_pad, tw);
+    columns_fft<cx, M, true>(Z1, NSP, tw);
     __syncthreads();
-    store_cols(Y1 + (size_t)n * M * M, Z1, S, cs, M);
+    store_cols_fixed<cx, M, NSP>(Y1 + (size_t)n * M * M, Z1, cs);
 }
 
 template <typename real, int M, int G>
@@ -845,11 +889,12 @@ __global__ void __launch_bounds__(256) kr_boxD(typename Cplx<real>::type *__rest
     const int n = blockIdx.y;
     if (threadIdx.x == 0) make_slots(cs, blockIdx.x * G, G, M);
     __syncthreads();
-    const int ns_pad = ((cs.ns + WG - 1) / WG) * WG;
+    constexpr int NSP = 2 * G;
+    static_assert(NSP % WG == 0, "slot count must be a multiple of the thread groups per warp");
     cx *W = tw + M;
-    load_cols_nat<cx, M>(W, Y2 + (size_t)n * M * M, cs, ns_pad);
+    load_cols_fixed<cx, M, NSP>(W, Y2 + (size_t)n * M * M, cs);
     __syncthreads();
-    columns_fft<cx, M, false>(W, ns_pad, tw);
+    columns_fft<cx, M, false>(W, NSP, tw);
     __syncthreads();
     const real dtk = (real)(a.dt * a.kfac);
     for_pairs(cs, M, [&](int sa, int ka, int sb, int kb) {
@@ -873,9 +918,9 @@ __global__ void __launch_bounds__(256) kr_boxD(typename Cplx<real>::type *__rest
         if (!(sa == sb && ka == kb)) W[(size_t)sb * S + kb] = hb;
     });
     __syncthreads();
-    columns_fft<cx, M, true>(W, ns_pad, tw);
+    columns_fft<cx, M, true>(W, NSP, tw);
     __syncthreads();
-    store_cols(Y1 + (size_t)n * M * M, W, S, cs, M);
+    store_cols_fixed<cx, M, NSP>(Y1 + (size_t)n * M * M, W, cs);
 }
 
 // ---- phi update (cell_phase_functions.cpp:126-217) + normals
@@ -931,6 +976,107 @@ __global__ void kf_update(const real *__restrict__ phi, real *__restrict__ phin,
           ((real)f0[n] - (real)P.beta * Tc + (real)P.eta * LT / q4 - (real)P.beta_lum_cells * hl[c] +
            (real)P.eta_lum_cells * Ll / q4 - (real)P.beta_ECM_cells * he[c] + (real)P.eta_ECM_cells * Le / q4);
     phin[o] = pn;
+}
+
+// kf_update on shared-memory tiles: a block is a UR x UC tile of one cell's
+// zone + ring (region W x W, W = 2z+2); phi, rho, T = psi - hfunc, h(lum) and
+// h(ECM) are staged with a one-site halo, so T is formed once per site and
+// the stencils read shared memory.  Normals on sites whose periodic ghost map
+// is not the identity (a region touching the grid's ghost ring) read their
+// mapped neighbours from global memory.
+constexpr int UR = 16, UC = 64;
+template <typename real>
+__global__ void __launch_bounds__(256) kf_update_tiled(const real *__restrict__ phi, real *__restrict__ phin,
+                                                       const real *__restrict__ rho, const real *__restrict__ hfunc,
+                                                       const double *__restrict__ f0, const real *__restrict__ psi,
+                                                       const real *__restrict__ hl, const real *__restrict__ he,
+                                                       const int *__restrict__ xc, const int *__restrict__ yc,
+                                                       DevParams P, real *__restrict__ Jc) {
+    constexpr int HR = UR + 2, HC = UC + 2;
+    __shared__ real sphi[HR][HC], srho[HR][HC], sT[HR][HC], shl[HR][HC], she[HR][HC];
+    const int n = blockIdx.z, N = P.N, z = P.zone, W = 2 * z + 2;
+    const int r0 = blockIdx.y * UR, c0 = blockIdx.x * UC;        // region-local tile origin
+    const int gi0 = xc[n] - z - 1 + r0, gj0 = yc[n] - z - 1 + c0;  // global origin
+    const size_t NN = (size_t)N * N, base = (size_t)n * NN;
+    for (int e = threadIdx.x; e < HR * HC; e += blockDim.x) {
+        const int a = e / HC, b = e - a * HC;
+        const int gi = min(max(gi0 - 1 + a, 0), N - 1), gj = min(max(gj0 - 1 + b, 0), N - 1);
+        const size_t k = (size_t)gi * N + gj;
+        sphi[a][b] = phi[base + k];
+        srho[a][b] = rho[base + k];
+        sT[a][b] = psi[k] - hfunc[base + k];
+        shl[a][b] = hl[k];
+        she[a][b] = he[k];
+    }
+    __syncthreads();
+    const real dx = (real)P.dx, dt = (real)P.dt, tau = (real)P.tau, sigma = (real)P.sigma;
+    const real c4 = (real)(1.0 / P.dx / P.dx / 4.0), inv2dx = (real)(1.0 / (2.0 * P.dx));
+    const real q4 = (real)4.0 * dx * dx;
+    const real fn0 = (real)f0[n];
+    real *Jx = Jc + (size_t)n * 2 * W * W, *Jy = Jx + (size_t)W * W;
+    for (int e = threadIdx.x; e < UR * UC; e += blockDim.x) {
+        const int li = e / UC, lj = e - li * UC;
+        const int rr = r0 + li, cc = c0 + lj;
+        if (rr >= W || cc >= W) continue;
+        const int gi = gi0 + li, gj = gj0 + lj;
+        const int a = li + 1, b = lj + 1;                         // shared coordinates
+        real ja, jb, g;
+        if (gi >= 1 && gi <= N - 2 && gj >= 1 && gj <= N - 2) {
+            ja = sphi[a + 1][b] - sphi[a - 1][b];
+            jb = sphi[a][b + 1] - sphi[a][b - 1];
+        } else {
+            const size_t c = (size_t)ghost_src(gi, N) * N + ghost_src(gj, N);
+            const real *p = phi + base;
+            ja = p[c + N] - p[c - N];
+            jb = p[c + 1] - p[c - 1];
+        }
+        g = sqrt(c4 * (ja * ja + jb * jb));
+        const size_t jo = (size_t)rr * W + cc;
+        const size_t o = base + (size_t)gi * N + gj;
+        const real f = sphi[a][b];
+        real pn = f;
+        if constexpr (sizeof(real) == 8) {
+            // FP64: the reference's operation order, divisions included
+            Jx[jo] = (g > (real)0.0) ? inv2dx * ja / g : (real)0.0;
+            Jy[jo] = (g > (real)0.0) ? inv2dx * jb / g : (real)0.0;
+            if (rr < 1 || rr > 2 * z || cc < 1 || cc > 2 * z) { phin[o] = f; continue; }
+            if (g > (real)0.0) {
+                pn -= (real)P.cpl / tau * (dt / dx / dx / (real)4.0) *
+                      exp(-(f - (real)0.5) * (f - (real)0.5) / (real)2.0 / sigma / sigma) / sqrt((real)(2.0 * M_PI)) /
+                      sigma * ((srho[a + 1][b] - srho[a - 1][b]) * ja + (srho[a][b + 1] - srho[a][b - 1]) * jb) / g;
+            }
+        } else {
+            // FP32: constant factors folded, one reciprocal of |grad phi|
+            const real rg = (g > (real)0.0) ? (real)1.0 / g : (real)0.0;
+            Jx[jo] = inv2dx * ja * rg;
+            Jy[jo] = inv2dx * jb * rg;
+            if (rr < 1 || rr > 2 * z || cc < 1 || cc > 2 * z) { phin[o] = f; continue; }
+            if (g > (real)0.0) {
+                const real d = f - (real)0.5;
+                pn -= (real)P.k_cpl * __expf(-d * d * (real)P.inv_2s2) *
+                      ((srho[a + 1][b] - srho[a - 1][b]) * ja + (srho[a][b + 1] - srho[a][b - 1]) * jb) * rg;
+            }
+        }
+        const real Tc = sT[a][b];
+        const real LT = lap9<real>(Tc, sT[a + 1][b], sT[a - 1][b], sT[a][b + 1], sT[a][b - 1], sT[a + 1][b + 1],
+                                   sT[a + 1][b - 1], sT[a - 1][b - 1], sT[a - 1][b + 1]);
+        const real Ll = lap9<real>(shl[a][b], shl[a + 1][b], shl[a - 1][b], shl[a][b + 1], shl[a][b - 1],
+                                   shl[a + 1][b + 1], shl[a + 1][b - 1], shl[a - 1][b - 1], shl[a - 1][b + 1]);
+        const real Le = lap9<real>(she[a][b], she[a + 1][b], she[a - 1][b], she[a][b + 1], she[a][b - 1],
+                                   she[a + 1][b + 1], she[a + 1][b - 1], she[a - 1][b - 1], she[a - 1][b + 1]);
+        if constexpr (sizeof(real) == 8) {
+            pn += ((real)1.0 / tau) * f * ((real)1.0 - f) * dt *
+                  (fn0 - (real)P.beta * Tc + (real)P.eta * LT / q4 - (real)P.beta_lum_cells * shl[a][b] +
+                   (real)P.eta_lum_cells * Ll / q4 - (real)P.beta_ECM_cells * she[a][b] +
+                   (real)P.eta_ECM_cells * Le / q4);
+        } else {
+            const real iq4 = (real)P.inv_q4;
+            pn += (real)P.dt_tau * f * ((real)1.0 - f) *
+                  (fn0 - (real)P.beta * Tc + (real)P.eta * LT * iq4 - (real)P.beta_lum_cells * shl[a][b] +
+                   (real)P.eta_lum_cells * Ll * iq4 - (real)P.beta_ECM_cells * she[a][b] + (real)P.eta_ECM_cells * Le * iq4);
+        }
+        phin[o] = pn;
+    }
 }
 
 // ---- persistent reshaping of all cells (cell_phase_functions.cpp:461-579)
@@ -1453,6 +1599,8 @@ BoxArgs box_args(pfag_ctx *c) {
     a.N = c->N; a.z = c->zone; a.M = c->M; a.logm = F(c)->logm; a.Ntot = c->Ntot;
     a.c4 = 1.0 / d.dx / d.dx / 4.0; a.sigma = d.sigma; a.dt = d.dt; a.kfac = d.kfac; a.friction = d.friction;
     a.dx = d.dx;
+    a.inv_2s2 = 1.0 / (2.0 * d.sigma * d.sigma);
+    a.k_delta = 1.0 / (std::sqrt(2.0 * M_PI) * d.sigma);
     for (int k = 0; k < 3; k++) {
         a.deg[k] = d.deg[k]; a.gen[k] = d.gen[k]; a.a_ort[k] = d.a_ort[k]; a.a_tan[k] = d.a_tan[k];
         a.visc[k] = d.visc[k]; a.bb[k] = d.bb[k];
@@ -1696,10 +1844,11 @@ struct Fused {
         // 6. phi update + normals, then reshaping
         {
             const int W = 2 * z + 2;
-            dim3 tb(32, 8), gb((W + 31) / 32, (W + 7) / 8, Nt);
+            dim3 gb((W + UC - 1) / UC, (W + UR - 1) / UR, Nt);
             pfag_prof_begin(c, "kf_update");
-            kf_update<real><<<gb, tb, 0, s>>>(R(c->phi), R(c->phin), R(c->rho), R(c->hfunc), c->d_f0, R(c->psi),
-                                              R(c->hlum), R(c->hecm), c->d_xc, c->d_yc, c->dp, R(r->Jc));
+            kf_update_tiled<real><<<gb, 256, 0, s>>>(R(c->phi), R(c->phin), R(c->rho), R(c->hfunc), c->d_f0,
+                                                     R(c->psi), R(c->hlum), R(c->hecm), c->d_xc, c->d_yc, c->dp,
+                                                     R(r->Jc));
             PFAG_LAUNCHED(c);
         }
         PFAG_CUDA_CHECK(cudaMemsetAsync(r->cK, 0, sizeof(int) * 3 * Nt, s));
@@ -1743,9 +1892,10 @@ struct Fused {
         cudaStream_t s = c->stream;
         const int Nt = c->Ntot;
         const size_t cs = sizeof(cx);
-        const size_t smA = (MM + (size_t)BG::ROWS * MM) * cs + (size_t)BG::ROWS * MM * (sizeof(real) + 1);
+        const size_t smA = (MM + (size_t)BG::ROWS * MM) * cs + (size_t)BG::ROWS * MM * sizeof(real) +
+                           (size_t)BG::ROWS * (MM + 4);
         const size_t smC = (MM + (size_t)BG::ROWS * MM) * cs;
-        const int nsB = ((2 * GB + BG::WG - 1) / BG::WG) * BG::WG, nsD = ((2 * GD + BG::WG - 1) / BG::WG) * BG::WG;
+        const int nsB = 2 * GB, nsD = 2 * GD;
         const size_t smB = (MM + 2 * (size_t)nsB * (MM + 1)) * cs;
         const size_t smD = (MM + (size_t)nsD * (MM + 1)) * cs;
         static bool configured = false;

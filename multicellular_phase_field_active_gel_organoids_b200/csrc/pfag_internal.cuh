@@ -59,6 +59,11 @@ struct DevParams {
     double thr_lum;             // rdev_threshold*rtol*rdt
     double rdev0_lum;           // rdev_ini*rtol*rdt
     double kfac;                // 2.0*M_PI/((2*zone_size-2)*dx)
+    // folded constants of the FP32 fused kernels
+    double k_cpl;               // coupling_PF_AG/tau*(dt/dx/dx/4)/sqrt(2 pi)/sigma
+    double inv_2s2;             // 1/(2 sigma^2)
+    double dt_tau;              // dt/tau
+    double inv_q4;              // 1/(4 dx^2)
     double inv_norm;            // 1/(M*M) as the reference divides: x/((2z-2)*(2z-2))
     // parameter maps, index 0 apical, 1 basal, 2 lateral
     double deg[3], gen[3], a_ort[3], a_tan[3], visc[3], bb[3];
