@@ -55,9 +55,10 @@ struct FusedRes {
     double *part_l;         // [2][coop_l]
     int *cK, *cdone, *ccnt; // per cell
     int *lK, *ldone, *lcnt; // [2] lumen, ECM
-    int tpc, tiles_i, tiles_j;
+    int tpc;                // reshaping strips per cell
     int resh_threads;       // block size of the reshaping kernel (one thread per zone column)
-    size_t resh_smem;       // its per-warp, per-cell partial sums
+    size_t resh_smem;       // its per-warp, per-cell partial sums + strip tile
+    size_t resh_tile;       // one staged strip (3 (RB+2) W reals)
     int npsi;
     int coop_r, coop_l;     // co-resident block counts of the persistent kernels
     int logm, rows_blk, grp_cols;
@@ -104,6 +105,35 @@ __device__ __forceinline__ double warp_sum_fixed(const volatile double *p, int n
     for (int k = l; k < n; k += 32) a += p[k];
     for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
     return a;
+}
+
+// Asynchronous global -> shared copy of one 4- or 8-byte element (no
+// register staging); cp_async_wait_all waits for this thread's copies.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src) {
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "element size");
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(sizeof(T)) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// True when every cell has a convergence stamp in (0, upto]; each warp reads
+// the stamps in parallel (32 per round) and votes.
+__device__ __forceinline__ bool all_done_upto(const int *done, int ncells, int upto) {
+    bool ok = true;
+    for (int base = 0; base < ncells; base += 32) {
+        const int n = base + (threadIdx.x & 31);
+        bool mine = true;
+        if (n < ncells) {
+            const int d = *(volatile const int *)&done[n];
+            mine = d != 0 && d <= upto;
+        }
+        ok = __all_sync(0xffffffffu, mine) && ok;
+        if (!ok) break;
+    }
+    return ok;
 }
 
 // ---- support-rectangle centroid (find_centres_cells, useful_functions.cpp:193-227)
@@ -596,7 +626,7 @@ template <int M> struct BoxGeom {
 
 // Pass A on register FFTs: one thread group per box row.
 template <typename real, int M>
-__global__ void __launch_bounds__(256) kr_boxA(const real *__restrict__ phi, const real *__restrict__ rho,
+__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxA(const real *__restrict__ phi, const real *__restrict__ rho,
                                                const real *__restrict__ lum, const real *__restrict__ ecm,
                                                const int *__restrict__ xc, const int *__restrict__ yc, BoxArgs a,
                                                typename Cplx<real>::type *__restrict__ Y1,
@@ -686,7 +716,7 @@ __global__ void __launch_bounds__(256) kr_boxA(const real *__restrict__ phi, con
 
 // Pass C on register FFTs.
 template <typename real, int M>
-__global__ void __launch_bounds__(256) kr_boxC(const typename Cplx<real>::type *__restrict__ Y1,
+__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxC(const typename Cplx<real>::type *__restrict__ Y1,
                                                typename Cplx<real>::type *__restrict__ Y2,
                                                const real *__restrict__ rho, const int *__restrict__ xc,
                                                const int *__restrict__ yc, BoxArgs a, real *__restrict__ vdx,
@@ -737,7 +767,7 @@ __global__ void __launch_bounds__(256) kr_boxC(const typename Cplx<real>::type *
 
 // Pass E on register FFTs.
 template <typename real, int M>
-__global__ void __launch_bounds__(256) kr_boxE(const typename Cplx<real>::type *__restrict__ Y1,
+__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxE(const typename Cplx<real>::type *__restrict__ Y1,
                                                const real *__restrict__ rho, const real *__restrict__ Rb,
                                                real *__restrict__ rhon, const int *__restrict__ xc,
                                                const int *__restrict__ yc, BoxArgs a) {
@@ -925,59 +955,6 @@ __global__ void __launch_bounds__(256) kr_boxD(typename Cplx<real>::type *__rest
 
 // ---- phi update (cell_phase_functions.cpp:126-217) + normals
 //      (useful_functions.cpp:356-388 with the periodic ghost map of :391-420)
-template <typename real>
-__global__ void kf_update(const real *__restrict__ phi, real *__restrict__ phin, const real *__restrict__ rho,
-                          const real *__restrict__ hfunc, const double *__restrict__ f0,
-                          const real *__restrict__ psi, const real *__restrict__ hl, const real *__restrict__ he,
-                          const int *__restrict__ xc, const int *__restrict__ yc, DevParams P,
-                          real *__restrict__ Jc) {
-    const int n = blockIdx.z, N = P.N, z = P.zone, W = 2 * z + 2;
-    const int ii = blockIdx.y * blockDim.y + threadIdx.y, jj = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ii >= W || jj >= W) return;
-    const int gi = xc[n] - z - 1 + ii, gj = yc[n] - z - 1 + jj;
-    const size_t NN = (size_t)N * N, base = (size_t)n * NN;
-    const real *p = phi + base;
-    const real dx = (real)P.dx;
-    const real c4 = (real)(1.0 / P.dx / P.dx / 4.0), inv2dx = (real)(1.0 / (2.0 * P.dx));
-    {
-        const int si = ghost_src(gi, N), sj = ghost_src(gj, N);
-        const size_t c = (size_t)si * N + sj;
-        const real a = p[c + N] - p[c - N], b = p[c + 1] - p[c - 1];
-        const real g = sqrt(c4 * (a * a + b * b));
-        real *J = Jc + (size_t)n * 2 * W * W;
-        J[(size_t)ii * W + jj] = (g > (real)0.0) ? inv2dx * a / g : (real)0.0;
-        J[(size_t)W * W + (size_t)ii * W + jj] = (g > (real)0.0) ? inv2dx * b / g : (real)0.0;
-    }
-    const size_t c = (size_t)gi * N + gj, o = base + c;
-    const bool in_zone = ii >= 1 && ii <= 2 * z && jj >= 1 && jj <= 2 * z;
-    if (!in_zone) { phin[o] = p[c]; return; }
-    const real dt = (real)P.dt, tau = (real)P.tau, sigma = (real)P.sigma;
-    const real f = p[c];
-    const real a = p[c + N] - p[c - N], b = p[c + 1] - p[c - 1];
-    const real gg = sqrt(c4 * (a * a + b * b));
-    real pn = f;
-    if (gg > (real)0.0) {
-        const real *r = rho + base;
-        pn -= (real)P.cpl / tau * (dt / dx / dx / (real)4.0) *
-              exp(-(f - (real)0.5) * (f - (real)0.5) / (real)2.0 / sigma / sigma) / sqrt((real)(2.0 * M_PI)) / sigma *
-              ((r[c + N] - r[c - N]) * a + (r[c + 1] - r[c - 1]) * b) / gg;
-    }
-    const real *hh = hfunc + base;
-    auto T = [&](size_t k) { return psi[k] - hh[k]; };
-    const real Tc = T(c);
-    const real LT = lap9<real>(Tc, T(c + N), T(c - N), T(c + 1), T(c - 1), T(c + N + 1), T(c + N - 1),
-                               T(c - N - 1), T(c - N + 1));
-    const real Ll = lap9<real>(hl[c], hl[c + N], hl[c - N], hl[c + 1], hl[c - 1], hl[c + N + 1], hl[c + N - 1],
-                               hl[c - N - 1], hl[c - N + 1]);
-    const real Le = lap9<real>(he[c], he[c + N], he[c - N], he[c + 1], he[c - 1], he[c + N + 1], he[c + N - 1],
-                               he[c - N - 1], he[c - N + 1]);
-    const real q4 = (real)4.0 * dx * dx;
-    pn += ((real)1.0 / tau) * f * ((real)1.0 - f) * dt *
-          ((real)f0[n] - (real)P.beta * Tc + (real)P.eta * LT / q4 - (real)P.beta_lum_cells * hl[c] +
-           (real)P.eta_lum_cells * Ll / q4 - (real)P.beta_ECM_cells * he[c] + (real)P.eta_ECM_cells * Le / q4);
-    phin[o] = pn;
-}
-
 // kf_update on shared-memory tiles: a block is a UR x UC tile of one cell's
 // zone + ring (region W x W, W = 2z+2); phi, rho, T = psi - hfunc, h(lum) and
 // h(ECM) are staged with a one-site halo, so T is formed once per site and
@@ -1081,131 +1058,93 @@ __global__ void __launch_bounds__(256) kf_update_tiled(const real *__restrict__ 
 
 // ---- persistent reshaping of all cells (cell_phase_functions.cpp:461-579)
 struct ReshArgs {
-    int N, z, Ntot, tpc, tiles_i, tiles_j, cap, rimax;
+    int N, z, Ntot, tpc, cap, rimax;   // tpc: strips per cell
+    int it0;                  // first iteration the persistent kernel runs
     double A, B, scale, thr;
     int *K, *done, *cnt;
     double *part;
     unsigned *err;
 };
 
-template <typename real>
-__global__ void kf_reshape(real *__restrict__ phi, real *__restrict__ phin, const real *__restrict__ Jc,
-                           const int *__restrict__ xc, const int *__restrict__ yc, ReshArgs a) {
-    cg::grid_group grid = cg::this_grid();
-    const int N = a.N, z = a.z, W = 2 * z + 2;
-    const real A = (real)a.A, B = (real)a.B;
+// One reshaping strip of cell n (cell_phase_functions.cpp:486-552): zone
+// rows [strip*RB, strip*RB + RB) of Q = P + F(P), one thread per zone column
+// (blockDim >= 2z).  P's strip with its one-row, one-column ring and the
+// normals' strip are staged in shared memory `sm` (3 (RB+2) W reals,
+// W = 2z + 2) and the 3x3 / cross stencils read them there.  Returns this
+// thread's sum of |Q - P| dx^2 / N_current (cell_phase_functions.cpp:554-561).
+// The caller synchronises the block before reusing `sm`.
+template <typename real, int RB>
+__device__ __forceinline__ double resh_tile(const real *__restrict__ P, real *__restrict__ Q,
+                                            const real *__restrict__ Jc, const int *__restrict__ xc,
+                                            const int *__restrict__ yc, const ReshArgs &a, int n, int strip,
+                                            real A, real B, real *sm) {
+    const int N = a.N, z = a.z, Z = 2 * z, W = Z + 2;
     const size_t NN = (size_t)N * N;
-    const int total = a.Ntot * a.tpc;
-    __shared__ int s_last, s_skip;
-    for (int it = 1; it <= a.cap; it++) {
-        real *P = (it & 1) ? phin : phi;
-        real *Q = (it & 1) ? phi : phin;
-        for (int t = blockIdx.x; t < total; t += gridDim.x) {
-            const int n = t / a.tpc, tile = t - n * a.tpc;
-            // a cell converged at iteration d is skipped from iteration d+1 on
-            if (threadIdx.x == 0) {
-                const int d = *(volatile int *)&a.done[n];
-                s_skip = (d != 0 && d < it);
+    const int zi0 = xc[n] - z, zj0 = yc[n] - z;
+    const int li0 = strip * RB;
+    const int nr = min(RB, Z - li0);
+    real *sP = sm, *sX = sm + (RB + 2) * W, *sY = sX + (RB + 2) * W;
+    const real *p = P + (size_t)n * NN + (size_t)(zi0 + li0 - 1) * N + (zj0 - 1);
+    const real *Jx = Jc + (size_t)n * 2 * W * W + (size_t)li0 * W, *Jy = Jx + (size_t)W * W;
+    for (int c = threadIdx.x; c < W; c += blockDim.x) {
+#pragma unroll
+        for (int r = 0; r < RB + 2; r++) {
+            if (r < nr + 2) {
+                cp_async_elem(sP + r * W + c, p + (size_t)r * N + c);
+                cp_async_elem(sX + r * W + c, Jx + (size_t)r * W + c);
+                cp_async_elem(sY + r * W + c, Jy + (size_t)r * W + c);
             }
-            __syncthreads();
-            const bool skip = s_skip;
-            __syncthreads();
-            if (skip) continue;
-            const int zi0 = xc[n] - z, zj0 = yc[n] - z;
-            const real *Jx = Jc + (size_t)n * 2 * W * W, *Jy = Jx + (size_t)W * W;
-            const real *p = P + (size_t)n * NN;
-            real *q = Q + (size_t)n * NN;
-            double acc = 0.0;
-            const int li_end = min(2 * z, (tile + 1) * RT_I);
-            for (int li = tile * RT_I; li < li_end; li++)
-              for (int lj = threadIdx.x; lj < 2 * z; lj += blockDim.x) {
-                const int gi = zi0 + li, gj = zj0 + lj;
-                const size_t c = (size_t)gi * N + gj;
-                const int ci = li + 1, cj = lj + 1;   // compact index of the site (ring at 0)
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    double acc = 0.0;
+    const int j = threadIdx.x;
+    if (j < Z) {
+        real *q = Q + (size_t)n * NN + (size_t)(zi0 + li0) * N + zj0 + j;
+        const int c = j + 1;
+#pragma unroll
+        for (int r = 0; r < RB; r++) {
+            if (r < nr) {
+                const int o = (r + 1) * W + c;
                 real w[3][3];
-                for (int u = 0; u < 3; u++)
-                    for (int v = 0; v < 3; v++) w[u][v] = p[c + (size_t)(u - 1) * N + (v - 1)];
-                const size_t jc = (size_t)ci * W + cj;
+#pragma unroll
+                for (int di = 0; di < 3; di++)
+#pragma unroll
+                    for (int dj = 0; dj < 3; dj++) w[di][dj] = sP[o + (di - 1) * W + dj - 1];
                 const real old = w[1][1];
-                const real nv = resh_update<real>(A, B, w, Jx[jc], Jx[jc + W], Jx[jc - W], Jx[jc + 1], Jx[jc - 1],
-                                                  Jy[jc], Jy[jc + W], Jy[jc - W], Jy[jc + 1], Jy[jc - 1], old);
-                q[c] = nv;
+                const real nv = resh_update<real>(A, B, w, sX[o], sX[o + W], sX[o - W], sX[o + 1], sX[o - 1], sY[o],
+                                                  sY[o + W], sY[o - W], sY[o + 1], sY[o - 1], old);
+                q[(size_t)r * N] = nv;
                 acc += fabs((double)nv - (double)old) * a.scale;
             }
-            const double bs = block_sum_d(acc);
-            if (threadIdx.x == 0) {
-                a.part[(size_t)n * a.tpc + tile] = bs;
-                __threadfence();
-                const int ticket = atomicAdd(&a.cnt[n], 1);
-                s_last = (ticket == a.tpc - 1);
-            }
-            __syncthreads();
-            if (s_last && threadIdx.x < 32) {
-                __threadfence();
-                const double rdev = warp_sum_fixed(a.part + (size_t)n * a.tpc, a.tpc);
-                if (threadIdx.x == 0) {
-                const int done_iters = a.K[n] + 1;
-                a.K[n] = done_iters;
-                bool stop = false;
-                if (done_iters - 1 > a.rimax) { atomicOr(a.err, ERRBIT_RELAX); stop = true; }
-                if (rdev <= a.thr) stop = true;
-                if (!stop && it == a.cap) { atomicOr(a.err, ERRBIT_ITER_CAP); stop = true; }
-                if (stop) a.done[n] = it;
-                a.cnt[n] = 0;
-                }
-            }
-            __syncthreads();
         }
-        grid.sync();
-        // stamps of the next iteration are > it, so a block that reads late
-        // cannot see a later convergence: every block takes the same decision
-        bool all = true;
-        for (int n = 0; n < a.Ntot && all; n++) {
-            const int d = *(volatile int *)&a.done[n];
-            all = (d != 0 && d <= it);
-        }
-        if (all) break;
     }
-    // odd iteration counts leave the last iterate in phi; the reference keeps
-    // the penultimate one there (the copy at the top of its loop), which is in phin
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int n = t / a.tpc, tile = t - n * a.tpc;
-        if (!(a.K[n] & 1)) continue;
-        const int zi0 = xc[n] - z, zj0 = yc[n] - z;
-        const int li_end = min(2 * z, (tile + 1) * RT_I);
-        for (int li = tile * RT_I; li < li_end; li++)
-            for (int lj = threadIdx.x; lj < 2 * z; lj += blockDim.x) {
-                const size_t o = (size_t)n * NN + (size_t)(zi0 + li) * N + zj0 + lj;
-                phi[o] = phin[o];
-            }
-    }
+    return acc;
 }
 
-// Persistent reshaping of all cells (cell_phase_functions.cpp:461-579),
-// register-blocked: a tile is one strip of RI zone rows of one cell, one thread
-// per zone column (blockDim = 32 * ceil(2z/32)); a thread holds its column of
-// the strip plus one halo row each side and takes the left/right neighbours
-// from the adjacent lanes (explicit loads at the warp edges).  Threads past
-// the zone width clamp their loads to the ring column and store nothing.
-// rdev: each warp adds its tiles' sums into its own shared slot per cell (its
-// tiles in a fixed order), the block writes per-cell partials, and after a
+// Persistent reshaping of all cells (cell_phase_functions.cpp:461-579) from
+// iteration a.it0 on; a task is one strip of one cell (resh_tile).
+// rdev: each warp adds its tasks' sums into its own shared slot per cell (its
+// tasks in a fixed order), the block writes per-cell partials, and after a
 // grid barrier one warp per cell sums the blocks' partials in block order and
-// takes the loop decision; a second barrier publishes it.
-constexpr int RESH_MAX_THREADS = 384;   // 3 warps per SM sub-partition at <= 168 registers
-template <typename real, int RI>
+// takes the loop decision; a second barrier publishes it.  done[n] holds the
+// iteration at which cell n stopped, so a block that reads it late still
+// agrees on the iteration count.
+constexpr int RESH_MAX_THREADS = 384;
+template <typename real, int RB>
 __global__ void __launch_bounds__(RESH_MAX_THREADS) kf_reshape_strips(real *__restrict__ phi, real *__restrict__ phin, const real *__restrict__ Jc,
                                   const int *__restrict__ xc, const int *__restrict__ yc, ReshArgs a) {
     cg::grid_group grid = cg::this_grid();
-    extern __shared__ double wacc[];          // [warps][Ntot]
-    const int N = a.N, z = a.z, Z = 2 * z, W = Z + 2;
+    extern __shared__ double wacc[];          // [warps][Ntot], then the strip tile
     const real A = (real)a.A, B = (real)a.B;
-    const size_t NN = (size_t)N * N;
     const int strips = a.tpc;
     const int total = a.Ntot * strips;
-    const int j = threadIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const bool active_col = j < Z;
-    const int jl = min(j, Z);                 // zone-local column of the loads (Z is the ring)
-    for (int it = 1; it <= a.cap; it++) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    real *tile = reinterpret_cast<real *>(wacc + nw * a.Ntot);
+    // iterations before it0 ran as separate kernels: nothing left to do?
+    if (all_done_upto(a.done, a.Ntot, a.it0 - 1)) return;
+    for (int it = a.it0; it <= a.cap; it++) {
         real *P = (it & 1) ? phin : phi;
         real *Q = (it & 1) ? phi : phin;
         for (int k = threadIdx.x; k < nw * a.Ntot; k += blockDim.x) wacc[k] = 0.0;
@@ -1214,83 +1153,11 @@ __global__ void __launch_bounds__(RESH_MAX_THREADS) kf_reshape_strips(real *__re
             const int n = t / strips, strip = t - n * strips;
             const int d = *(volatile int *)&a.done[n];   // not written during this phase
             if (d != 0 && d < it) continue;
-            const int zi0 = xc[n] - z, zj0 = yc[n] - z;
-            const int li0 = strip * RI;
-            const int nr = min(RI, Z - li0);
-            const int gj = zj0 + jl;
-            const real *p = P + (size_t)n * NN;
-            const real *Jx = Jc + (size_t)n * 2 * W * W, *Jy = Jx + (size_t)W * W;
-            real pc[RI + 2], pl[RI + 2], pr[RI + 2];
-            real xc_[RI + 2], yc_[RI + 2], xl[RI], xr[RI], yl[RI], yr[RI];
-#pragma unroll
-            for (int r = 0; r < RI + 2; r++) {
-                const int li = min(li0 - 1 + r, Z);           // -1 .. Z (ring rows)
-                pc[r] = p[(size_t)(zi0 + li) * N + gj];
-                const size_t jc = (size_t)(li + 1) * W + (jl + 1);
-                xc_[r] = Jx[jc];
-                yc_[r] = Jy[jc];
-            }
-#pragma unroll
-            for (int r = 0; r < RI + 2; r++) {
-                pl[r] = __shfl_up_sync(0xffffffffu, pc[r], 1);
-                pr[r] = __shfl_down_sync(0xffffffffu, pc[r], 1);
-            }
-#pragma unroll
-            for (int r = 0; r < RI; r++) {
-                xl[r] = __shfl_up_sync(0xffffffffu, xc_[r + 1], 1);
-                xr[r] = __shfl_down_sync(0xffffffffu, xc_[r + 1], 1);
-                yl[r] = __shfl_up_sync(0xffffffffu, yc_[r + 1], 1);
-                yr[r] = __shfl_down_sync(0xffffffffu, yc_[r + 1], 1);
-            }
-            if (lane == 0) {            // left neighbour column jl - 1 >= -1 (ring)
-#pragma unroll
-                for (int r = 0; r < RI + 2; r++) {
-                    const int li = min(li0 - 1 + r, Z);
-                    pl[r] = p[(size_t)(zi0 + li) * N + gj - 1];
-                }
-#pragma unroll
-                for (int r = 0; r < RI; r++) {
-                    const int li = min(li0 + r, Z);
-                    const size_t jc = (size_t)(li + 1) * W + jl;
-                    xl[r] = Jx[jc];
-                    yl[r] = Jy[jc];
-                }
-            }
-            if (lane == 31) {           // right neighbour column min(jl + 1, Z)
-                const int jr = min(jl + 1, Z);
-#pragma unroll
-                for (int r = 0; r < RI + 2; r++) {
-                    const int li = min(li0 - 1 + r, Z);
-                    pr[r] = p[(size_t)(zi0 + li) * N + zj0 + jr];
-                }
-#pragma unroll
-                for (int r = 0; r < RI; r++) {
-                    const int li = min(li0 + r, Z);
-                    const size_t jc = (size_t)(li + 1) * W + jr + 1;
-                    xr[r] = Jx[jc];
-                    yr[r] = Jy[jc];
-                }
-            }
-            double acc = 0.0;
-            real *q = Q + (size_t)n * NN;
-#pragma unroll
-            for (int r = 0; r < RI; r++) {
-                if (r < nr && active_col) {
-                    real w[3][3];
-                    w[0][0] = pl[r];     w[0][1] = pc[r];     w[0][2] = pr[r];
-                    w[1][0] = pl[r + 1]; w[1][1] = pc[r + 1]; w[1][2] = pr[r + 1];
-                    w[2][0] = pl[r + 2]; w[2][1] = pc[r + 2]; w[2][2] = pr[r + 2];
-                    const real old = w[1][1];
-                    const real nv = resh_update<real>(A, B, w, xc_[r + 1], xc_[r + 2], xc_[r], xr[r], xl[r],
-                                                      yc_[r + 1], yc_[r + 2], yc_[r], yr[r], yl[r], old);
-                    q[(size_t)(zi0 + li0 + r) * N + gj] = nv;
-                    acc += fabs((double)nv - (double)old) * a.scale;
-                }
-            }
+            double acc = resh_tile<real, RB>(P, Q, Jc, xc, yc, a, n, strip, A, B, tile);
             for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
             if (lane == 0) wacc[warp * a.Ntot + n] += acc;
+            __syncthreads();
         }
-        __syncthreads();
         for (int n = threadIdx.x; n < a.Ntot; n += blockDim.x) {
             double sum = 0.0;
             for (int w2 = 0; w2 < nw; w2++) sum += wacc[w2 * a.Ntot + n];
@@ -1314,24 +1181,55 @@ __global__ void __launch_bounds__(RESH_MAX_THREADS) kf_reshape_strips(real *__re
             }
         }
         grid.sync();
-        bool all = true;
-        for (int n = 0; n < a.Ntot && all; n++) {
-            const int d = *(volatile int *)&a.done[n];
-            all = (d != 0 && d <= it);
-        }
-        if (all) break;
+        if (all_done_upto(a.done, a.Ntot, it)) break;
     }
-    // odd iteration counts leave the last iterate in phi; the reference keeps
-    // the penultimate one there (the copy at the top of its loop), which is in phin
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int n = t / strips, strip = t - n * strips;
-        if (!(a.K[n] & 1) || !active_col) continue;
-        const int zi0 = xc[n] - z, zj0 = yc[n] - z;
-        const int li_end = min(Z, (strip + 1) * RI);
-        for (int li = strip * RI; li < li_end; li++) {
-            const size_t o = (size_t)n * NN + (size_t)(zi0 + li) * N + zj0 + j;
-            phi[o] = phin[o];
-        }
+}
+
+// Reshaping iteration 1 at full occupancy: one strip per block, per-strip
+// partial sums (block order of warps fixed).
+template <typename real, int RB>
+__global__ void __launch_bounds__(RESH_MAX_THREADS) kf_resh_first(const real *__restrict__ P, real *__restrict__ Q,
+                                                                   const real *__restrict__ Jc,
+                                                                   const int *__restrict__ xc,
+                                                                   const int *__restrict__ yc, ReshArgs a) {
+    extern __shared__ double tile_d[];
+    const int n = blockIdx.y, strip = blockIdx.x;
+    const double acc = resh_tile<real, RB>(P, Q, Jc, xc, yc, a, n, strip, (real)a.A, (real)a.B,
+                                           reinterpret_cast<real *>(tile_d));
+    const double bs = block_sum_d(acc);
+    if (threadIdx.x == 0) a.part[(size_t)n * a.tpc + strip] = bs;
+}
+
+// Loop decision after iteration `it` run by kf_resh_first: one warp per cell,
+// strips summed in order (cell_phase_functions.cpp:554-573).
+__global__ void kf_resh_decide(ReshArgs a, int it) {
+    const int n = blockIdx.x;
+    const double rdev = warp_sum_fixed(a.part + (size_t)n * a.tpc, a.tpc);
+    if (threadIdx.x == 0) {
+        const int k = a.K[n] + 1;
+        a.K[n] = k;
+        bool stop = false;
+        if (k - 1 > a.rimax) { atomicOr(a.err, ERRBIT_RELAX); stop = true; }
+        if (rdev <= a.thr) stop = true;
+        if (!stop && it == a.cap) { atomicOr(a.err, ERRBIT_ITER_CAP); stop = true; }
+        if (stop) a.done[n] = it;
+    }
+}
+
+// Odd iteration counts leave the last iterate in phi; the reference keeps the
+// penultimate one there (the copy at the top of its loop), which is in phin.
+template <typename real, int RB>
+__global__ void __launch_bounds__(RESH_MAX_THREADS) kf_resh_copy(real *__restrict__ phi, const real *__restrict__ phin,
+                                                                  const int *__restrict__ xc,
+                                                                  const int *__restrict__ yc, ReshArgs a) {
+    const int n = blockIdx.y, strip = blockIdx.x, j = threadIdx.x, Z = 2 * a.z;
+    if (!(a.K[n] & 1) || j >= Z) return;
+    const int zi0 = xc[n] - a.z, zj0 = yc[n] - a.z;
+    const size_t base = (size_t)n * a.N * a.N;
+    const int li_end = min(Z, (strip + 1) * RB);
+    for (int li = strip * RB; li < li_end; li++) {
+        const size_t o = base + (size_t)(zi0 + li) * a.N + zj0 + j;
+        phi[o] = phin[o];
     }
 }
 
@@ -1683,20 +1581,21 @@ struct Fused {
             pfag_set_error("fused path: zone width 2*%d above %d columns; use the plain path", c->zone, RESH_MAX_THREADS);
             return PFAG_E_UNSUPPORTED;
         }
-        r->resh_smem = (size_t)(r->resh_threads / 32) * c->Ntot * sizeof(double);
+        r->resh_tile = (size_t)3 * (RESH_RB + 2) * (2 * c->zone + 2) * sizeof(real);
+        r->resh_smem = (size_t)(r->resh_threads / 32) * c->Ntot * sizeof(double) + r->resh_tile;
         if (r->resh_smem > 200 * 1024) { pfag_set_error("too many cells for the reshaping kernel's per-warp sums"); return PFAG_E_UNSUPPORTED; }
-        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_reshape_strips<real, RESH_RI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_reshape_strips<real, RESH_RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)r->resh_smem));
-        PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kf_reshape_strips<real, RESH_RI>,
+        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_resh_first<real, RESH_RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)r->resh_tile));
+        PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kf_reshape_strips<real, RESH_RB>,
                                                                        r->resh_threads, r->resh_smem));
         if (per < 1) { pfag_set_error("reshaping kernel cannot be resident with %d threads", r->resh_threads); return PFAG_E_UNSUPPORTED; }
         r->coop_r = nsm * std::min(per, 8);
         PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kf_lum<real>, FT, 0));
         if (per < 1) { pfag_set_error("lumen/ECM kernel cannot be resident"); return PFAG_E_UNSUPPORTED; }
         r->coop_l = nsm * std::min(per, 4);
-        r->tiles_i = (2 * c->zone + RESH_RI - 1) / RESH_RI;
-        r->tiles_j = 1;
-        r->tpc = r->tiles_i;
+        r->tpc = (2 * c->zone + RESH_RB - 1) / RESH_RB;
         r->npsi = ((c->N + 31) / 32) * ((c->N + 31) / 32);
         return PFAG_OK;
     }
@@ -1854,17 +1753,29 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaMemsetAsync(r->cK, 0, sizeof(int) * 3 * Nt, s));
         {
             ReshArgs ra{};
-            ra.N = N; ra.z = z; ra.Ntot = Nt; ra.tpc = r->tpc; ra.tiles_i = r->tiles_i; ra.tiles_j = r->tiles_j;
+            ra.N = N; ra.z = z; ra.Ntot = Nt; ra.tpc = r->tpc;
             ra.rimax = c->p.rimax; ra.cap = c->relax_cap;
             ra.A = d.A_resh; ra.B = d.B_resh; ra.scale = d.dx * d.dx / (double)d.Ncur; ra.thr = d.thr_cells;
             ra.K = r->cK; ra.done = r->cdone; ra.cnt = r->ccnt; ra.part = r->part_r; ra.err = c->d_err;
             real *a0 = R(c->phi), *a1 = R(c->phin);
             const real *a2 = R(r->Jc);
             const int *a3 = c->d_xc, *a4 = c->d_yc;
+            ra.it0 = 2;
+            const dim3 gs(r->tpc, Nt);
+            pfag_prof_begin(c, "kf_resh_first");
+            kf_resh_first<real, RESH_RB><<<gs, r->resh_threads, r->resh_tile, s>>>(R(c->phin), R(c->phi), R(r->Jc), c->d_xc,
+                                                                        c->d_yc, ra);
+            PFAG_LAUNCHED(c);
+            pfag_prof_begin(c, "kf_resh_decide");
+            kf_resh_decide<<<Nt, 32, 0, s>>>(ra, 1);
+            PFAG_LAUNCHED(c);
             void *args[] = {&a0, &a1, (void *)&a2, (void *)&a3, (void *)&a4, &ra};
             pfag_prof_begin(c, "kf_reshape");
-            PFAG_TRY(launch_coop_t((const void *)kf_reshape_strips<real, RESH_RI>, &r->coop_r, r->resh_threads, args,
+            PFAG_TRY(launch_coop_t((const void *)kf_reshape_strips<real, RESH_RB>, &r->coop_r, r->resh_threads, args,
                                    r->resh_smem, s));
+            PFAG_LAUNCHED(c);
+            pfag_prof_begin(c, "kf_resh_copy");
+            kf_resh_copy<real, RESH_RB><<<gs, r->resh_threads, 0, s>>>(R(c->phi), R(c->phin), c->d_xc, c->d_yc, ra);
             PFAG_LAUNCHED(c);
         }
         // 7. rho <- rhon on the boxes, ghost ring
@@ -1879,8 +1790,8 @@ struct Fused {
         return PFAG_OK;
     }
 
-    // rows per reshaping strip (registers: ~10 reals per row and thread)
-    static constexpr int RESH_RI = 4;
+    // zone rows per reshaping strip
+    static constexpr int RESH_RB = 8;
 
     // primaries per block of the column passes (shared tile near 64 KB)
     static constexpr int GB = sizeof(real) == 8 ? 4 : 8;
@@ -1934,7 +1845,7 @@ struct Fused {
         const int Nt = c->Ntot;
         if (std::getenv("PFAG_DEBUG_COOP")) {
             cudaFuncAttributes fr{}, fl{};
-            cudaFuncGetAttributes(&fr, (const void *)kf_reshape_strips<real, RESH_RI>);
+            cudaFuncGetAttributes(&fr, (const void *)kf_reshape_strips<real, RESH_RB>);
             cudaFuncGetAttributes(&fl, (const void *)kf_lum<real>);
             std::fprintf(stderr, "pfag coop: reshape %d blocks x %d threads (%d regs), lum %d blocks x %d (%d regs)\n",
                          r->coop_r, r->resh_threads, fr.numRegs, r->coop_l, FT, fl.numRegs);
