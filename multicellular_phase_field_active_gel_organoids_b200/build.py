@@ -1,8 +1,12 @@
-"""Build libpfag.so (the CUDA kernels and the C ABI) for sm_100a, in-tree.
+"""Build libpfag.so (the CUDA kernels and the C ABI) for sm_100a, in-tree,
+and the drop-in libraries dropin/libpfag_dropin_fp{32,64}.so over it.
 
 nvcc -gencode arch=compute_100a,code=sm_100a -lineinfo -O3 ... -shared, linked
-against cuFFT (the plain comparison path) and the CUDA runtime.  The output
-lands next to this file so it travels with the source tree.
+against cuFFT (the plain comparison path) and the CUDA runtime.  The drop-in
+libraries (the reference's step functions with their C++ signatures, in float
+and in double) are host C++ compiled by g++ and linked against libpfag.so with
+an $ORIGIN-relative run path.  Everything lands next to this file so it travels
+with the source tree.
 """
 from __future__ import annotations
 
@@ -23,6 +27,33 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxe
 # 2^-54 staircase of the initial profile) identical.
 PER_FILE = {"pfag_plain.cu": ["-fmad=false"], "pfag_fused_f64.cu": ["-fmad=false"]}
 OBJ_DIR = os.path.join(HERE, "_build")
+DROPIN_SRC = os.path.join(HERE, "dropin", "pfag_dropin.cpp")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+
+
+def dropin_lib(precision: int) -> str:
+    return os.path.join(HERE, "dropin", f"libpfag_dropin_fp{precision}.so")
+
+
+def build_dropin(force: bool = False) -> list[str]:
+    """g++ the drop-in shim in float (fp32) and double (fp64)."""
+    out = []
+    inc = os.path.join(HERE, "..", "include")
+    for prec in (32, 64):
+        lib = dropin_lib(prec)
+        out.append(lib)
+        if not force and os.path.exists(lib) and os.path.getmtime(lib) >= max(
+                os.path.getmtime(DROPIN_SRC), os.path.getmtime(LIB)):
+            continue
+        cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall", "-Wno-unused-parameter",
+               *(["-DPFAG_DROPIN_DOUBLE"] if prec == 64 else []),
+               "-I", inc, "-I", os.path.join(CUDA_HOME, "include"), DROPIN_SRC, "-o", lib,
+               "-L", HERE, "-lpfag", "-Wl,-rpath,$ORIGIN/..",
+               "-L", os.path.join(CUDA_HOME, "lib64"), "-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("g++ failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    return out
 
 
 def sources() -> list[str]:
@@ -70,3 +101,4 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print("\n".join(build_dropin(force="--force" in sys.argv)))

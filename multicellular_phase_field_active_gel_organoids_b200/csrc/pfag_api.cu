@@ -172,6 +172,13 @@ int pfag_check_device_error(pfag_ctx *c) {
         return PFAG_E_ZONE;
     }
     if (e & ERRBIT_ITER_CAP) { pfag_set_error("a device relaxation loop hit its iteration cap"); return PFAG_E_RELAX; }
+    if (e & ERRBIT_RELAX) {
+        // a cell loop passed rimax: the reference prints and goes on
+        // (cell_phase_functions.cpp:563-567); counted, then cleared
+        c->stats.relax_failures++;
+        PFAG_CUDA_CHECK(cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), c->stream));
+        PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+    }
     return PFAG_OK;
 }
 

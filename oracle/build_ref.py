@@ -13,6 +13,10 @@ Compiles, with g++/gcc on the host,
     `double`; nothing else is changed.  This is the reference's own FP64 run.
   * this directory's C restatement pfag_oracle.c (the oracle "port") into
       oracle/lib/liboracle_fp32.so, oracle/lib/liboracle_fp64.so
+  * the reference's own main and host files linked against the package's
+    drop-in libraries (its step functions over the B200 library):
+      oracle/_ref/dropin_main_fp32, oracle/_ref/dropin_main_fp64
+    the harness of the drop-in test, not a checker.
 
 The reference build needs the reference checkout (default /root/reference,
 override with PFAG_REFERENCE_DIR); where it is absent the prebuilt files in
@@ -94,6 +98,72 @@ def _build_reference(ref: str, double: bool) -> None:
               *[o for o in objs if not o.endswith("ref_harness.cpp.o")], "-lm"])
 
 
+# Host files of the reference that stay in a drop-in build: everything but the
+# three step-function files that libpfag_dropin replaces.
+DROPIN_KEPT = ["initialisation_functions.cpp", "declare_tables.cpp", "declare_fft_tables.cpp"]
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+PKG = os.path.join(HERE, "..", "multicellular_phase_field_active_gel_organoids_b200")
+
+
+def _build_dropin_main(ref: str, double: bool) -> None:
+    """The reference's own main (main_code/run_with_active_gels.cpp) and its
+    host files, compiled as they are (float -> double rewritten for fp64) and
+    linked against the package's libpfag_dropin_fp{32,64}.so in place of
+    useful_functions.cpp, rho_functions.cpp and cell_phase_functions.cpp.
+    Parameters come from ref_params.cpp (PFAG_REF_PARAMS), real cuFFT headers
+    and library (main creates its two plans itself), an empty openacc.h."""
+    tag = "fp64" if double else "fp32"
+    with tempfile.TemporaryDirectory(prefix=f"pfag_dropin_{tag}_") as tmp:
+        src_funcs = os.path.join(ref, "functions")
+        src_main = os.path.join(ref, "main_code", "run_with_active_gels.cpp")
+        if double:
+            for name in DROPIN_KEPT + REF_HEADERS:
+                text = open(os.path.join(src_funcs, name)).read()
+                open(os.path.join(tmp, name), "w").write(re.sub(r"\bfloat\b", "double", text))
+            text = open(src_main).read()
+            open(os.path.join(tmp, "run_with_active_gels.cpp"), "w").write(re.sub(r"\bfloat\b", "double", text))
+            inc = tmp
+            srcs = [os.path.join(tmp, n) for n in DROPIN_KEPT] + [os.path.join(tmp, "run_with_active_gels.cpp")]
+        else:
+            inc = src_funcs
+            srcs = [os.path.join(src_funcs, n) for n in DROPIN_KEPT] + [src_main]
+        acc = os.path.join(tmp, "acc")
+        os.makedirs(acc)
+        open(os.path.join(acc, "openacc.h"), "w").write("/* empty: OpenACC pragmas are inert under g++ */\n")
+        defs = ["-DPFAG_REF_DOUBLE"] if double else []
+        incs = ["-I", acc, "-I", inc, "-I", os.path.join(CUDA_HOME, "include")]
+        objs = []
+        for src in srcs + [os.path.join(HERE, "ref_params.cpp")]:
+            obj = os.path.join(tmp, os.path.basename(src) + ".o")
+            _run(["g++", *CXXFLAGS, *defs, *incs, "-c", src, "-o", obj])
+            objs.append(obj)
+        dropin = os.path.abspath(os.path.join(PKG, "dropin"))
+        _run(["g++", "-o", os.path.join(REF_OUT, f"dropin_main_{tag}"), *objs,
+              "-L", dropin, f"-lpfag_dropin_{tag}", "-L", os.path.abspath(PKG), "-lpfag",
+              "-L", os.path.join(CUDA_HOME, "lib64"), "-lcufft", "-lcudart",
+              "-Wl,-rpath,$ORIGIN/../../multicellular_phase_field_active_gel_organoids_b200/dropin",
+              "-Wl,-rpath,$ORIGIN/../../multicellular_phase_field_active_gel_organoids_b200",
+              "-Wl,-rpath," + os.path.join(CUDA_HOME, "lib64"), "-lm"])
+
+
+def build_dropin_main(force: bool = False) -> bool:
+    """Build oracle/_ref/dropin_main_fp{32,64}; needs the reference checkout and
+    the package's drop-in libraries.  False when the checkout is absent."""
+    ref = reference_dir()
+    if ref is None:
+        return False
+    os.makedirs(REF_OUT, exist_ok=True)
+    for double in (False, True):
+        tag = "fp64" if double else "fp32"
+        out = os.path.join(REF_OUT, f"dropin_main_{tag}")
+        lib = os.path.join(PKG, "dropin", f"libpfag_dropin_{tag}.so")
+        if not os.path.exists(lib):
+            raise RuntimeError(f"{lib} is missing: build the package first")
+        if force or not os.path.exists(out):
+            _build_dropin_main(ref, double)
+    return True
+
+
 def build_reference(force: bool = False) -> bool:
     """Build oracle/_ref from the reference checkout; False when it is absent."""
     ref = reference_dir()
@@ -127,6 +197,8 @@ def main() -> int:
     force = "--force" in sys.argv
     build_port(force)
     ok = build_reference(force)
+    if ok:
+        build_dropin_main(force)
     print("oracle port built;", "reference built" if ok else "reference checkout absent (prebuilt files kept)")
     return 0
 

@@ -147,3 +147,36 @@ def run_reference(params: dict, init, nsteps: int, precision: str = "fp64", star
     if status != "ok":
         raise RuntimeError("reference run failed: " + val)
     return val
+
+
+def main_binary(kind: str, precision: str = "fp64") -> str:
+    """oracle/_ref/{ref_main,dropin_main}_fp{32,64}: the reference's own main
+    linked with its step files (ref_main) or with the package's drop-in
+    libraries (dropin_main)."""
+    return os.path.join(HERE, "_ref", f"{kind}_{precision}")
+
+
+def run_main_binary(binary: str, params: dict, init, workdir: str, env: dict | None = None,
+                    timeout: float = 600.0):
+    """Run a build of the reference's main in `workdir`: write the parameter
+    file and the ini_*.bin state files of `init` = (phi, rho, lum, ECM), run
+    Nsteps steps as main does, and return the state of the last snapshot slot
+    read back from the ini_*.bin files main writes (phi, rho, lum, ECM), with
+    the process's stderr."""
+    import subprocess
+    import sys
+    sys.path.insert(0, os.path.dirname(HERE))
+    from multicellular_phase_field_active_gel_organoids_b200 import fileio, params as P
+    prec = 64 if binary.endswith("fp64") else 32
+    os.makedirs(os.path.join(workdir, "data_int"), exist_ok=True)
+    pfile = os.path.join(workdir, "params.txt")
+    P.write_param_file(params, pfile)
+    fileio.write_state_files(workdir, *init, precision=prec)
+    e = dict(os.environ)
+    e["PFAG_REF_PARAMS"] = pfile
+    e.update(env or {})
+    r = subprocess.run([binary], cwd=workdir, env=e, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"{os.path.basename(binary)} exited with {r.returncode}:\n{r.stderr[-3000:]}")
+    n, N = int(params["N_ini"]), int(params["N_s"])
+    return fileio.read_state_files(workdir, n, N, prec), r.stderr
