@@ -19,7 +19,7 @@ int pfag_fused_alloc(pfag_ctx *c) {
 void pfag_fused_free(pfag_ctx *c) {
     FusedRes *r = F(c);
     if (!r) return;
-    if (r->graph_ok) { cudaGraphExecDestroy(r->gexec); cudaGraphDestroy(r->graph); }
+    fused_drop_graph(r);
     void *bufs[] = {r->Y1, r->Y2, r->Rb, r->clsT, r->Jc, r->Jl, r->rect, r->part_s, r->part_r, r->part_e, r->part_l,
                     r->cK};
     for (void *b : bufs) if (b) cudaFree(b);

@@ -63,10 +63,14 @@ struct FusedRes {
     int coop_r, coop_l;     // co-resident block counts of the persistent kernels
     int logm, rows_blk, grp_cols;
     size_t smemA, smemB, smemC, smemD, smemE;
+    // one step captured as a CUDA graph after the first eager step
     cudaGraph_t graph;
     cudaGraphExec_t gexec;
     bool graph_ok;
-    int graph_it;           // steps in the captured graph (1)
+    int graph_state;        // 0 not tried, 1 captured, -1 capture failed (eager from then on)
+    long graph_key;         // host inputs the capture depends on (relaxation cap)
+    long graph_launches;    // kernel launches in one replay
+    long eager_steps;
 };
 
 template <typename real>
@@ -1651,7 +1655,6 @@ struct Fused {
             pfag_set_error("initial zone leaves the grid or a cell is empty");
             return (c->h_err[0] & ERRBIT_EMPTY_CELL) ? PFAG_E_EMPTY_CELL : PFAG_E_ZONE;
         }
-        r->graph_ok = false;
         return PFAG_OK;
     }
 
@@ -1870,9 +1873,54 @@ struct Fused {
 // Entry points instantiated once per precision (pfag_fused_f64.cu, pfag_fused_f32.cu).
 template <typename real> int fused_alloc_t(pfag_ctx *c) { return Fused<real>(c).alloc(); }
 template <typename real> int fused_upload_t(pfag_ctx *c) { return Fused<real>(c).upload_hook(); }
+inline void fused_drop_graph(FusedRes *r) {
+    if (r->graph_ok) { cudaGraphExecDestroy(r->gexec); cudaGraphDestroy(r->graph); }
+    r->graph_ok = false;
+}
+
+// One step.  The first step runs eagerly (kernel attributes and the
+// persistent kernels' block counts settle there); the next one is captured
+// into a CUDA graph that every later step replays with one launch.  Profiling,
+// debug capture and PFAG_NO_GRAPH keep the eager path; a failed capture falls
+// back to it for good.
 template <typename real> int fused_step_t(pfag_ctx *c, bool sync_host) {
-    int rc = Fused<real>(c).enqueue();
-    if (rc != PFAG_OK) return rc;
+    FusedRes *r = F(c);
+    const bool graphable = !pfag_prof_on(c) && !c->debug && !std::getenv("PFAG_NO_GRAPH");
+    const long key = (long)c->relax_cap;
+    if (r->graph_ok && (!graphable || r->graph_key != key)) {
+        fused_drop_graph(r);
+        r->graph_state = 0;
+    }
+    if (graphable && r->graph_state == 0 && r->eager_steps >= 1) {
+        cudaStream_t s = c->stream;
+        const long l0 = c->launches;
+        r->graph_state = -1;
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const int rc = Fused<real>(c).enqueue();
+            cudaGraph_t g = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(s, &g);
+            if (rc == PFAG_OK && e == cudaSuccess && g && cudaGraphInstantiate(&r->gexec, g, 0) == cudaSuccess) {
+                r->graph = g;
+                r->graph_ok = true;
+                r->graph_state = 1;
+                r->graph_key = key;
+                r->graph_launches = c->launches - l0;
+            } else if (g) {
+                cudaGraphDestroy(g);
+            }
+        }
+        c->launches = l0;
+        (void)cudaGetLastError();   // a refused capture leaves a non-sticky error
+    }
+    int rc = PFAG_OK;
+    if (r->graph_ok) {
+        PFAG_CUDA_CHECK(cudaGraphLaunch(r->gexec, c->stream));
+        c->launches += r->graph_launches;
+    } else {
+        rc = Fused<real>(c).enqueue();
+        if (rc != PFAG_OK) return rc;
+        r->eager_steps++;
+    }
     if (sync_host) {
         PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
         rc = Fused<real>(c).stats();

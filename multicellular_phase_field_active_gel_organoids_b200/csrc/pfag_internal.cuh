@@ -116,6 +116,7 @@ struct pfag_ctx {
 void pfag_prof_begin(pfag_ctx *ctx, const char *name);
 void pfag_prof_end(pfag_ctx *ctx);
 void pfag_prof_free(pfag_ctx *ctx);
+bool pfag_prof_on(pfag_ctx *ctx);
 
 // Launch accounting helper; closes the profiling bracket of the launch.
 #define PFAG_LAUNCHED(ctx) ((ctx)->launches++, pfag_prof_end(ctx))

@@ -48,6 +48,8 @@ void pfag_prof_free(pfag_ctx *c) {
     c->prof = nullptr;
 }
 
+bool pfag_prof_on(pfag_ctx *c) { return c && c->prof && PS(c)->on; }
+
 extern "C" int pfag_set_profile(pfag_ctx *c, int on) {
     if (!c) return PFAG_E_ARG;
     if (!c->prof) c->prof = new ProfState();
