@@ -162,24 +162,33 @@ def kernel_bytes(cfg, precision: int, iters: dict) -> dict:
     box = n * M * M
     zone = n * (2 * z) * (2 * z)
     ring = n * Wz * Wz
+    lum_it = max(iters.get("lum_iters", 1), 1)
+    ecm_it = max(iters.get("ecm_iters", 1), 1)
+    cell_it = max(iters.get("cell_iters_sum", n), n)
     out = {
         # reads phi (centre), phi_{n-1}, phi_{n+1}, rho, lum, ECM; writes pi_xx+i pi_yy, pi_xy, R, class byte
         "kf_boxA": box * (6 * w + 5 * w + 1),
         "kf_boxB": box * (4 * w + 1 + 2 * w),
         "kf_boxC": box * (2 * w + w + 2 * w),
         "kf_boxD": box * (2 * w + 2 * w),
+        # reads Y1, rho, R; writes rho in place
         "kf_boxE": box * (2 * w + w + w + w),
         # reads phi, rho, hfunc, psi, h(lum), h(ECM); writes phin, J_x, J_y
         "kf_update": ring * 9 * w,
-        # per iteration: read P and J (x, y), write Q, over each active cell's zone
-        "kf_reshape": (2 * z) * (2 * z) * 4 * w * max(iters.get("cell_iters_sum", n), 1),
+        # reshaping iteration 1: read P and J (x, y), write Q, over every zone
+        "kf_resh_first": zone * 4 * w,
+        # further iterations, per launch
+        "kf_reshape": (2 * z) * (2 * z) * 4 * w * (cell_it - n),
         "kf_psi": N * N * (2 * w + 3 * w) + zone * w,
         "kf_hfunc_area": zone * 2 * w,
         "kf_centroid": zone * w,
-        "kf_rho_copy": box * 2 * w,
-        # update (read lum, ECM, psi, h's, write lumn, ECMn), normals (read 4, write 4),
-        # per relaxation iteration (read P, Jx, Jy, write Q) for each field
-        "kf_lum": N * N * w * (7 + 8 + 4 * max(iters.get("lum_iters", 1) + iters.get("ecm_iters", 1), 1)),
+        # read lum, ECM, psi, h(lum), h(ECM); write lumn, ECMn
+        "kfl_update": N * N * 7 * w,
+        # read lum, lumn, ECM, ECMn; write 4 normal components
+        "kfl_normals": N * N * 8 * w,
+        # per launch (two launches per step): read P, Jx, Jy, write Q per active field
+        "kl_relax": N * N * 4 * w * (min(lum_it, 2) + min(ecm_it, 2)) // 2,
+        "kf_lum": N * N * 4 * w * (max(lum_it - 2, 0) + max(ecm_it - 2, 0)),
     }
     return out
 

@@ -21,7 +21,7 @@ void pfag_fused_free(pfag_ctx *c) {
     if (!r) return;
     fused_drop_graph(r);
     void *bufs[] = {r->Y1, r->Y2, r->Rb, r->clsT, r->Jc, r->Jl, r->rect, r->part_s, r->part_r, r->part_e, r->part_l,
-                    r->cK};
+                    r->part_lt, r->cK};
     for (void *b : bufs) if (b) cudaFree(b);
     delete r;
     c->fused = nullptr;

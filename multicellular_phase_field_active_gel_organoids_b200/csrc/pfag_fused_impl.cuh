@@ -59,6 +59,9 @@ struct FusedRes {
     int resh_threads;       // block size of the reshaping kernel (one thread per zone column)
     size_t resh_smem;       // its per-warp, per-cell partial sums + strip tile
     size_t resh_tile;       // one staged strip (3 (RB+2) W reals)
+    int ntl;                // lumen/ECM relaxation tiles per field (LRB rows x FT columns)
+    size_t lum_tile;        // their staged tile (3 (LRB+2) (FT+2) reals)
+    double *part_lt;        // [2][ntl] tile partial sums
     int npsi;
     int coop_r, coop_l;     // co-resident block counts of the persistent kernels
     int logm, rows_blk, grp_cols;
@@ -146,11 +149,31 @@ __global__ void kf_centroid(const real *__restrict__ phi, const int4 *__restrict
                             long long *__restrict__ acc) {
     const int n = blockIdx.y;
     const int4 r = rect[n];
-    long long cnt = 0, sx = 0, sy = 0;
     const real *p = phi + (size_t)n * N * N;
-    for (int i = r.x + blockIdx.x; i < r.y; i += gridDim.x)
-        for (int j = r.z + threadIdx.x; j < r.w; j += blockDim.x)
-            if (p[(size_t)i * N + j] > (real)0.5) { cnt++; sx += i; sy += j; }
+    // CR rows x 2 column slots per thread per round, all loads issued first
+    constexpr int CR = 4;
+    int c32 = 0, sx32 = 0, sy32 = 0;
+    long long cnt = 0, sx = 0, sy = 0;
+    for (int jb = r.z + threadIdx.x; jb < r.w; jb += 2 * blockDim.x)
+    for (int ib = r.x + blockIdx.x; ib < r.y; ib += CR * gridDim.x) {
+        const int j0 = jb, j1 = jb + blockDim.x;
+        real v0[CR], v1[CR];
+#pragma unroll
+        for (int k = 0; k < CR; k++) {
+            const int i = ib + k * gridDim.x;
+            v0[k] = (i < r.y && j0 < r.w) ? p[(size_t)i * N + j0] : (real)0.0;
+            v1[k] = (i < r.y && j1 < r.w) ? p[(size_t)i * N + j1] : (real)0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < CR; k++) {
+            const int i = ib + k * gridDim.x;
+            if (v0[k] > (real)0.5) { c32++; sx32 += i; sy32 += j0; }
+            if (v1[k] > (real)0.5) { c32++; sx32 += i; sy32 += j1; }
+        }
+        // int partials stay far from overflow: at most 2 CR sites of index < 2^15 per round
+        cnt += c32; sx += sx32; sy += sy32;
+        c32 = sx32 = sy32 = 0;
+    }
     for (int o = 16; o > 0; o >>= 1) {
         cnt += __shfl_down_sync(0xffffffffu, cnt, o);
         sx += __shfl_down_sync(0xffffffffu, sx, o);
@@ -201,18 +224,37 @@ __global__ void kf_hfunc_area(const real *__restrict__ phi, real *__restrict__ h
     const int zi0 = xc[n] - z, zj0 = yc[n] - z;
     const size_t base = (size_t)n * N * N;
     double acc = 0.0;
-    for (int i = r.x + blockIdx.x; i < r.y; i += gridDim.x)
-      for (int j = r.z + threadIdx.x; j < r.w; j += blockDim.x) {
-        const size_t o = base + (size_t)i * N + j;
-        real h;
-        if (i >= zi0 && i < zi0 + 2 * z && j >= zj0 && j < zj0 + 2 * z) {
-            const real f = phi[o];
-            h = f * f * ((real)3.0 - (real)2.0 * f);
-            hfunc[o] = h;
-        } else {
-            h = hfunc[o];
-        }
-        acc += (double)h * dx2;
+    // CR rows x 2 column slots per thread per round, all loads issued first;
+    // inside the zone h is formed from phi and stored, outside it is read
+    constexpr int CR = 4;
+    for (int jb = r.z + threadIdx.x; jb < r.w; jb += 2 * blockDim.x)
+    for (int ib = r.x + blockIdx.x; ib < r.y; ib += CR * gridDim.x) {
+        const int js[2] = {jb, jb + (int)blockDim.x};
+        real v[CR][2];
+        bool inz[CR][2], ok[CR][2];
+#pragma unroll
+        for (int k = 0; k < CR; k++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const int i = ib + k * gridDim.x, j = js[c];
+                ok[k][c] = i < r.y && j < r.w;
+                inz[k][c] = i >= zi0 && i < zi0 + 2 * z && j >= zj0 && j < zj0 + 2 * z;
+                v[k][c] = ok[k][c] ? (inz[k][c] ? phi[base + (size_t)i * N + j] : hfunc[base + (size_t)i * N + j])
+                                   : (real)0.0;
+            }
+#pragma unroll
+        for (int k = 0; k < CR; k++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                if (!ok[k][c]) continue;
+                const int i = ib + k * gridDim.x, j = js[c];
+                real h = v[k][c];
+                if (inz[k][c]) {
+                    h = h * h * ((real)3.0 - (real)2.0 * h);
+                    hfunc[base + (size_t)i * N + j] = h;
+                }
+                acc += (double)h * dx2;
+            }
     }
     double s = block_sum_d(acc);
     if (threadIdx.x == 0) part[(size_t)n * gridDim.x + blockIdx.x] = s;
@@ -268,10 +310,22 @@ __global__ void kf_psi(const real *__restrict__ hfunc, const int4 *__restrict__ 
         const int i = ti0 + (e >> 5), j = tj0 + (e & 31);
         if (i >= N || j >= N) continue;
         const size_t s = (size_t)i * N + j;
+        // cells in list order, 8 loads in flight; a cell whose B_n misses the
+        // site contributes an exact 0 (as hfunc_cell does there)
         real sum = (real)0.0;
-        for (int q = 0; q < nl; q++) {
-            const int4 r = lrect[q];
-            if (i >= r.x && i < r.y && j >= r.z && j < r.w) sum += hfunc[(size_t)list[q] * N * N + s];
+        for (int q0 = 0; q0 < nl; q0 += 8) {
+            real v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int q = q0 + u;
+                v[u] = (real)0.0;
+                if (q < nl) {
+                    const int4 r = lrect[q];
+                    if (i >= r.x && i < r.y && j >= r.z && j < r.w) v[u] = hfunc[(size_t)list[q] * N * N + s];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) sum += v[u];
         }
         psi[s] = sum;
         const real a = lum[s], b = ecm[s];
@@ -593,8 +647,8 @@ __global__ void kf_boxD(typename Cplx<real>::type *__restrict__ Y1, const typena
 }
 
 template <typename real>
-__global__ void kf_boxE(const typename Cplx<real>::type *__restrict__ Y1, const real *__restrict__ rho,
-                        const real *__restrict__ Rb, real *__restrict__ rhon, const int *__restrict__ xc,
+__global__ void kf_boxE(const typename Cplx<real>::type *__restrict__ Y1, const real *rho,
+                        const real *__restrict__ Rb, real *rhon, const int *__restrict__ xc,
                         const int *__restrict__ yc, BoxArgs a, int R) {
     typedef typename Cplx<real>::type cx;
     extern __shared__ unsigned char smraw[];
@@ -772,8 +826,8 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxC(const 
 // Pass E on register FFTs.
 template <typename real, int M>
 __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxE(const typename Cplx<real>::type *__restrict__ Y1,
-                                               const real *__restrict__ rho, const real *__restrict__ Rb,
-                                               real *__restrict__ rhon, const int *__restrict__ xc,
+                                               real *__restrict__ rho, const real *__restrict__ Rb,
+                                               const int *__restrict__ xc,
                                                const int *__restrict__ yc, BoxArgs a) {
     typedef typename Cplx<real>::type cx;
     typedef RegFFT<cx, M> RF;
@@ -794,12 +848,22 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxE(const 
     RF::template run<true>(v, t, scr + g * M, tw);
     const real mm = (real)((double)M * (double)M), dt = (real)a.dt;
     const size_t so = (size_t)n * N * N + (size_t)(bi + i) * N + bj;
+    // rho is updated in place: all loads of the row segment before the stores
+    real old[E1], rb[E1];
 #pragma unroll
     for (int r = 0; r < RF::R2; r++)
 #pragma unroll
         for (int k2 = 0; k2 < TT; k2++) {
             const int k = RF::out_index(t, r, k2);
-            rhon[so + k] = rho[so + k] + dt * Rb[rowo + k] + v[r * TT + k2].x / mm;
+            old[r * TT + k2] = rho[so + k];
+            rb[r * TT + k2] = Rb[rowo + k];
+        }
+#pragma unroll
+    for (int r = 0; r < RF::R2; r++)
+#pragma unroll
+        for (int k2 = 0; k2 < TT; k2++) {
+            const int k = RF::out_index(t, r, k2);
+            rho[so + k] = old[r * TT + k2] + dt * rb[r * TT + k2] + v[r * TT + k2].x / mm;
         }
 }
 
@@ -1103,6 +1167,8 @@ __device__ __forceinline__ double resh_tile(const real *__restrict__ P, real *__
     cp_async_wait_all();
     __syncthreads();
     double acc = 0.0;
+    float facc = 0.0f;
+    const ReshConst kc = resh_const(a.A, a.B);
     const int j = threadIdx.x;
     if (j < Z) {
         real *q = Q + (size_t)n * NN + (size_t)(zi0 + li0) * N + zj0 + j;
@@ -1117,13 +1183,21 @@ __device__ __forceinline__ double resh_tile(const real *__restrict__ P, real *__
 #pragma unroll
                     for (int dj = 0; dj < 3; dj++) w[di][dj] = sP[o + (di - 1) * W + dj - 1];
                 const real old = w[1][1];
-                const real nv = resh_update<real>(A, B, w, sX[o], sX[o + W], sX[o - W], sX[o + 1], sX[o - 1], sY[o],
-                                                  sY[o + W], sY[o - W], sY[o + 1], sY[o - 1], old);
-                q[(size_t)r * N] = nv;
-                acc += fabs((double)nv - (double)old) * a.scale;
+                if constexpr (sizeof(real) == 4) {
+                    const float nv = resh_update_f(kc, w, sX[o], sX[o + W], sX[o - W], sX[o + 1], sX[o - 1], sY[o],
+                                                   sY[o + W], sY[o - W], sY[o + 1], sY[o - 1], old);
+                    q[(size_t)r * N] = nv;
+                    facc += fabsf(nv - old);
+                } else {
+                    const real nv = resh_update<real>(A, B, w, sX[o], sX[o + W], sX[o - W], sX[o + 1], sX[o - 1],
+                                                      sY[o], sY[o + W], sY[o - W], sY[o + 1], sY[o - 1], old);
+                    q[(size_t)r * N] = nv;
+                    acc += fabs((double)nv - (double)old) * a.scale;
+                }
             }
         }
     }
+    if constexpr (sizeof(real) == 4) acc = (double)facc * a.scale;
     return acc;
 }
 
@@ -1192,7 +1266,7 @@ __global__ void __launch_bounds__(RESH_MAX_THREADS) kf_reshape_strips(real *__re
 // Reshaping iteration 1 at full occupancy: one strip per block, per-strip
 // partial sums (block order of warps fixed).
 template <typename real, int RB>
-__global__ void __launch_bounds__(RESH_MAX_THREADS) kf_resh_first(const real *__restrict__ P, real *__restrict__ Q,
+__global__ void __maxnreg__(72) kf_resh_first(const real *__restrict__ P, real *__restrict__ Q,
                                                                    const real *__restrict__ Jc,
                                                                    const int *__restrict__ xc,
                                                                    const int *__restrict__ yc, ReshArgs a) {
@@ -1241,6 +1315,7 @@ __global__ void __launch_bounds__(RESH_MAX_THREADS) kf_resh_copy(real *__restric
 //      (cell_phase_functions.cpp:372-444, :709-871; useful_functions.cpp:422-462)
 struct LumArgs {
     int N, cap, rimax, npsi;
+    int it0;           // first iteration the persistent kernel runs
     double dx, dt, tau_lum, xi_lum, beta_lum_cells, eta_lum_cells, beta_lum_ECM;
     double alpha_ECM, tau_ECM, xi_ECM, beta_ECM_cells, eta_ECM_cells;
     double A, B, thr, rdev0;
@@ -1331,7 +1406,13 @@ __global__ void kf_lum(real *__restrict__ lum, real *__restrict__ lumn, real *__
     const int lane = threadIdx.x & 31;
     const int tiles_i = (N + LRI - 1) / LRI, tiles_j = (N + blockDim.x - 1) / blockDim.x;
     const int ntiles = tiles_i * tiles_j;
-    for (int it = 1; it <= a.cap; it++) {
+    // iterations before it0 ran as separate kernels: nothing left to do?
+    if (threadIdx.x < 32 && all_done_upto(a.done, 2, a.it0 - 1)) s_skip = 1;
+    else if (threadIdx.x == 0) s_skip = 0;
+    __syncthreads();
+    if (s_skip) return;
+    __syncthreads();
+    for (int it = a.it0; it <= a.cap; it++) {
         for (int f = 0; f < 2; f++) {
             if (threadIdx.x == 0) {
                 const int d = *(volatile int *)&a.done[f];
@@ -1401,8 +1482,12 @@ __global__ void kf_lum(real *__restrict__ lum, real *__restrict__ lumn, real *__
                             w[0][0] = pl[r];     w[0][1] = pc[r];     w[0][2] = pr[r];
                             w[1][0] = pl[r + 1]; w[1][1] = pc[r + 1]; w[1][2] = pr[r + 1];
                             w[2][0] = pl[r + 2]; w[2][1] = pc[r + 2]; w[2][2] = pr[r + 2];
-                            v = resh_update<real>(A, B, w, xc_[r + 1], xc_[r + 2], xc_[r], xr[r], xl[r], yc_[r + 1],
-                                                  yc_[r + 2], yc_[r], yr[r], yl[r], w[1][1]);
+                            if constexpr (sizeof(real) == 4)
+                                v = resh_update_f(resh_const(a.A, a.B), w, xc_[r + 1], xc_[r + 2], xc_[r], xr[r],
+                                                  xl[r], yc_[r + 1], yc_[r + 2], yc_[r], yr[r], yl[r], w[1][1]);
+                            else
+                                v = resh_update<real>(A, B, w, xc_[r + 1], xc_[r + 2], xc_[r], xr[r], xl[r],
+                                                      yc_[r + 1], yc_[r + 2], yc_[r], yr[r], yl[r], w[1][1]);
                         }
                         acc += fabs((double)v - (double)pc[r + 1]) * dx2;
                         Q[(size_t)ii * N + jj] = v;
@@ -1437,27 +1522,124 @@ __global__ void kf_lum(real *__restrict__ lum, real *__restrict__ lumn, real *__
         const int d0 = *(volatile int *)&a.done[0], d1 = *(volatile int *)&a.done[1];
         if (d0 != 0 && d0 <= it && d1 != 0 && d1 <= it) break;
     }
-    // the step ends with lum <- lumn: the last iterate is in lum for odd counts
-    for (int f = 0; f < 2; f++) {
-        if (a.K[f] & 1) continue;
-        real *dst = f ? ecm : lum;
-        const real *src = f ? ecmn : lumn;
-        for (int i = blockIdx.x; i < N; i += gridDim.x)
-            for (int j = threadIdx.x; j < N; j += blockDim.x) dst[(size_t)i * N + j] = src[(size_t)i * N + j];
+}
+
+// One relaxation iteration `it` of field f = blockIdx.y (0 lumen, 1 ECM;
+// cell_phase_functions.cpp:774-869) on a tile of LRB grid rows x blockDim
+// columns, with the field and its normals staged in shared memory (one-site
+// halo, clamped at the grid edge, where the Dirichlet sites take their side
+// values and no stencil).  Fields already converged return at once.  The
+// block's sum of |Q - P| dx^2 goes to part[f][block] (fixed order).
+constexpr int LRB = 8;
+template <typename real>
+__global__ void __launch_bounds__(256) kl_relax(real *__restrict__ lum, real *__restrict__ lumn,
+                                                real *__restrict__ ecm, real *__restrict__ ecmn,
+                                                const real *__restrict__ Jl, LumArgs a, int it,
+                                                double *__restrict__ part) {
+    extern __shared__ double lsm_d[];
+    const int f = blockIdx.y;
+    {
+        const int d = a.done[f];    // written only by kl_decide, between launches
+        if (d != 0 && d < it) return;
+    }
+    const int N = a.N;
+    const size_t NN = (size_t)N * N;
+    const int TB = blockDim.x, TW = TB + 2;
+    const int tiles_j = (N + TB - 1) / TB;
+    const int ti = blockIdx.x / tiles_j, tj = blockIdx.x - ti * tiles_j;
+    const int i0 = ti * LRB, j0 = tj * TB;
+    real *sP = reinterpret_cast<real *>(lsm_d), *sX = sP + (LRB + 2) * TW, *sY = sX + (LRB + 2) * TW;
+    const real *P = (it & 1) ? (f ? ecmn : lumn) : (f ? ecm : lum);
+    real *Q = (it & 1) ? (f ? ecm : lum) : (f ? ecmn : lumn);
+    const real *Jx = Jl + (size_t)(2 * f) * NN, *Jy = Jl + (size_t)(2 * f + 1) * NN;
+#pragma unroll
+    for (int r = 0; r < LRB + 2; r++) {
+        const size_t row = (size_t)min(max(i0 - 1 + r, 0), N - 1) * N;
+        for (int cc = threadIdx.x; cc < TW; cc += TB) {
+            const size_t k = row + min(max(j0 - 1 + cc, 0), N - 1);
+            cp_async_elem(sP + r * TW + cc, P + k);
+            cp_async_elem(sX + r * TW + cc, Jx + k);
+            cp_async_elem(sY + r * TW + cc, Jy + k);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const real A = (real)a.A, B = (real)a.B, side = f ? (real)1.0 : (real)0.0;
+    const ReshConst kc = resh_const(a.A, a.B);
+    const double dx2 = a.dx * a.dx;
+    const int jj = j0 + threadIdx.x;
+    double acc = 0.0;
+    float facc = 0.0f;
+    if (jj < N) {
+#pragma unroll
+        for (int r = 0; r < LRB; r++) {
+            const int ii = i0 + r;
+            if (ii < N) {
+                const int o = (r + 1) * TW + threadIdx.x + 1;
+                const real old = sP[o];
+                real v;
+                bool edge;
+                dirichlet_val<real>(ii, jj, N, side, (real)0.0, v, edge);
+                if (!edge) {
+                    real w[3][3];
+#pragma unroll
+                    for (int di = 0; di < 3; di++)
+#pragma unroll
+                        for (int dj = 0; dj < 3; dj++) w[di][dj] = sP[o + (di - 1) * TW + dj - 1];
+                    if constexpr (sizeof(real) == 4)
+                        v = resh_update_f(kc, w, sX[o], sX[o + TW], sX[o - TW], sX[o + 1], sX[o - 1], sY[o],
+                                          sY[o + TW], sY[o - TW], sY[o + 1], sY[o - 1], old);
+                    else
+                        v = resh_update<real>(A, B, w, sX[o], sX[o + TW], sX[o - TW], sX[o + 1], sX[o - 1], sY[o],
+                                              sY[o + TW], sY[o - TW], sY[o + 1], sY[o - 1], old);
+                }
+                if constexpr (sizeof(real) == 4) facc += fabsf(v - old);
+                else acc += fabs((double)v - (double)old) * dx2;
+                Q[(size_t)ii * N + jj] = v;
+            }
+        }
+    }
+    if constexpr (sizeof(real) == 4) acc = (double)facc * dx2;
+    const double bs = block_sum_d(acc);
+    if (threadIdx.x == 0) part[(size_t)f * gridDim.x + blockIdx.x] = bs;
+}
+
+// Loop decision after iteration `it` of kl_relax: one warp per field, the
+// tiles' partials summed in tile order (cell_phase_functions.cpp:851-868).
+__global__ void kl_decide(LumArgs a, int it, const double *__restrict__ part, int ntiles) {
+    const int f = blockIdx.x;
+    {
+        const int d = a.done[f];
+        if (d != 0 && d < it) return;
+    }
+    const double rdev = warp_sum_fixed(part + (size_t)f * ntiles, ntiles);
+    if (threadIdx.x == 0) {
+        const int k2 = a.K[f] + 1;
+        a.K[f] = k2;
+        bool stop = false;
+        if (k2 - 1 > a.rimax) { atomicOr(a.err, ERRBIT_RELAX); stop = true; }
+        if (rdev <= a.thr) stop = true;
+        if (!stop && it == a.cap) { atomicOr(a.err, ERRBIT_ITER_CAP); stop = true; }
+        if (stop) a.done[f] = it;
     }
 }
 
-// ---- end of step: rho <- rhon on the boxes, then the periodic ghost ring
+// The step ends with lum <- lumn, ECM <- ECMn (run_with_active_gels.cpp:179-181):
+// after an odd iteration count the last iterate already sits in lum / ECM.
 template <typename real>
-__global__ void kf_rho_copy(real *__restrict__ rho, const real *__restrict__ rhon, const int *__restrict__ xc,
-                            const int *__restrict__ yc, int N, int z, int M) {
-    const int n = blockIdx.z;
-    const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= M || j >= M) return;
-    const size_t o = (size_t)n * N * N + (size_t)(xc[n] - z + 1 + i) * N + (yc[n] - z + 1 + j);
-    rho[o] = rhon[o];
+__global__ void kl_copy(real *__restrict__ lum, const real *__restrict__ lumn, real *__restrict__ ecm,
+                        const real *__restrict__ ecmn, const int *__restrict__ K, int N) {
+    const int f = blockIdx.y;
+    if (K[f] & 1) return;
+    real *dst = f ? ecm : lum;
+    const real *src = f ? ecmn : lumn;
+    const size_t NN = (size_t)N * N;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < NN; k += (size_t)gridDim.x * blockDim.x)
+        dst[k] = src[k];
 }
 
+// ---- end of step: the periodic ghost ring of rho (boundary_conditions_cells,
+//      useful_functions.cpp:391-420, applied to rhon at rho_functions.cpp:469)
 template <typename real>
 __global__ void kf_rho_ring(real *__restrict__ rho, int N) {
     const int n = blockIdx.y;
@@ -1600,6 +1782,10 @@ struct Fused {
         if (per < 1) { pfag_set_error("lumen/ECM kernel cannot be resident"); return PFAG_E_UNSUPPORTED; }
         r->coop_l = nsm * std::min(per, 4);
         r->tpc = (2 * c->zone + RESH_RB - 1) / RESH_RB;
+        r->ntl = ((c->N + LRB - 1) / LRB) * ((c->N + FT - 1) / FT);
+        r->lum_tile = (size_t)3 * (LRB + 2) * (FT + 2) * sizeof(real);
+        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kl_relax<real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)r->lum_tile));
         r->npsi = ((c->N + 31) / 32) * ((c->N + 31) / 32);
         return PFAG_OK;
     }
@@ -1618,6 +1804,7 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_r, sizeof(double) * (size_t)c->Ntot * std::max(r->tpc, r->coop_r)));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_e, sizeof(double) * r->npsi));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_l, sizeof(double) * 2 * r->coop_l));
+        PFAG_CUDA_CHECK(cudaMalloc(&r->part_lt, sizeof(double) * 2 * r->ntl));
         PFAG_CUDA_CHECK(cudaMalloc(&r->cK, sizeof(int) * (3 * c->Ntot + 8)));
         r->cdone = r->cK + c->Ntot;
         r->ccnt = r->cK + 2 * c->Ntot;
@@ -1685,7 +1872,19 @@ struct Fused {
         kf_psi<real><<<dim3(tiles, tiles), FT, 0, s>>>(R(c->hfunc), r->rect, Nt, N, R(c->lum), R(c->ecm), R(c->psi),
                                                         R(c->hlum), R(c->hecm), d.dx * d.dx, r->part_e);
         PFAG_LAUNCHED(c);
-        // 4. spectral solve
+        // 4. phi update + normals on zone + ring (reads the old rho, like the
+        //    spectral solve, which therefore updates rho in place afterwards)
+        {
+            const int W = 2 * z + 2;
+            dim3 gb((W + UC - 1) / UC, (W + UR - 1) / UR, Nt);
+            pfag_prof_begin(c, "kf_update");
+            kf_update_tiled<real><<<gb, 256, 0, s>>>(R(c->phi), R(c->phin), R(c->rho), R(c->hfunc), c->d_f0,
+                                                     R(c->psi), R(c->hlum), R(c->hecm), c->d_xc, c->d_yc, c->dp,
+                                                     R(r->Jc));
+            PFAG_LAUNCHED(c);
+        }
+        // 5. spectral solve; pass E writes the new rho over each box in place
+        //    (rho <- rhon of run_with_active_gels.cpp:175-178 on the box)
         const BoxArgs ba = box_args(c);
         const int Rr = r->rows_blk, G = r->grp_cols;
         cx *Y1 = (cx *)r->Y1, *Y2 = (cx *)r->Y2;
@@ -1709,11 +1908,11 @@ struct Fused {
         pfag_prof_begin(c, "kf_boxD");
         kf_boxD<real><<<dim3(ngrp, Nt), FT, r->smemD, s>>>(Y1, Y2, ba, G); PFAG_LAUNCHED(c);
         pfag_prof_begin(c, "kf_boxE");
-        kf_boxE<real><<<dim3(M / Rr, Nt), FT, r->smemE, s>>>(Y1, R(c->rho), R(r->Rb), R(c->rhon), c->d_xc, c->d_yc,
+        kf_boxE<real><<<dim3(M / Rr, Nt), FT, r->smemE, s>>>(Y1, R(c->rho), R(r->Rb), R(c->rho), c->d_xc, c->d_yc,
                                                              ba, Rr);
         PFAG_LAUNCHED(c);
         }
-        // 5. lumen / ECM
+        // 6. lumen / ECM
         PFAG_CUDA_CHECK(cudaMemsetAsync(r->lK, 0, sizeof(int) * 8, s));
         {
             LumArgs la{};
@@ -1736,23 +1935,29 @@ struct Fused {
             pfag_prof_begin(c, "kfl_normals");
             kfl_normals<real><<<gb, tb, 0, s>>>(R(c->lum), R(c->lumn), R(c->ecm), R(c->ecmn), R(r->Jl), N, d.dx);
             PFAG_LAUNCHED(c);
+            // iterations 1 .. LUM_REGULAR as full-occupancy kernels, the rest (if
+            // any field is still moving) in the persistent kernel
+            for (int it = 1; it <= LUM_REGULAR; it++) {
+                pfag_prof_begin(c, "kl_relax");
+                kl_relax<real><<<dim3(r->ntl, 2), FT, r->lum_tile, s>>>(R(c->lum), R(c->lumn), R(c->ecm),
+                                                                         R(c->ecmn), R(r->Jl), la, it, r->part_lt);
+                PFAG_LAUNCHED(c);
+                pfag_prof_begin(c, "kl_decide");
+                kl_decide<<<2, 32, 0, s>>>(la, it, r->part_lt, r->ntl);
+                PFAG_LAUNCHED(c);
+            }
+            la.it0 = LUM_REGULAR + 1;
             real *a0 = R(c->lum), *a1 = R(c->lumn), *a2 = R(c->ecm), *a3 = R(c->ecmn);
             const real *a4 = R(r->Jl);
             void *args[] = {&a0, &a1, &a2, &a3, (void *)&a4, &la};
             pfag_prof_begin(c, "kf_lum");
             PFAG_TRY(launch_coop_t((const void *)kf_lum<real>, &r->coop_l, FT, args, 0, s));
             PFAG_LAUNCHED(c);
-        }
-        // 6. phi update + normals, then reshaping
-        {
-            const int W = 2 * z + 2;
-            dim3 gb((W + UC - 1) / UC, (W + UR - 1) / UR, Nt);
-            pfag_prof_begin(c, "kf_update");
-            kf_update_tiled<real><<<gb, 256, 0, s>>>(R(c->phi), R(c->phin), R(c->rho), R(c->hfunc), c->d_f0,
-                                                     R(c->psi), R(c->hlum), R(c->hecm), c->d_xc, c->d_yc, c->dp,
-                                                     R(r->Jc));
+            pfag_prof_begin(c, "kl_copy");
+            kl_copy<real><<<dim3(296, 2), FT, 0, s>>>(R(c->lum), R(c->lumn), R(c->ecm), R(c->ecmn), r->lK, N);
             PFAG_LAUNCHED(c);
         }
+        // 7. reshaping of the cells
         PFAG_CUDA_CHECK(cudaMemsetAsync(r->cK, 0, sizeof(int) * 3 * Nt, s));
         {
             ReshArgs ra{};
@@ -1781,11 +1986,8 @@ struct Fused {
             kf_resh_copy<real, RESH_RB><<<gs, r->resh_threads, 0, s>>>(R(c->phi), R(c->phin), c->d_xc, c->d_yc, ra);
             PFAG_LAUNCHED(c);
         }
-        // 7. rho <- rhon on the boxes, ghost ring
+        // 8. periodic ghost ring of rho
         {
-            dim3 tb(32, 8), gb((M + 31) / 32, (M + 7) / 8, Nt);
-            pfag_prof_begin(c, "kf_rho_copy");
-            kf_rho_copy<real><<<gb, tb, 0, s>>>(R(c->rho), R(c->rhon), c->d_xc, c->d_yc, N, z, M); PFAG_LAUNCHED(c);
             pfag_prof_begin(c, "kf_rho_ring");
             kf_rho_ring<real><<<dim3((4 * N + 255) / 256, Nt), 256, 0, s>>>(R(c->rho), N); PFAG_LAUNCHED(c);
         }
@@ -1795,6 +1997,8 @@ struct Fused {
 
     // zone rows per reshaping strip
     static constexpr int RESH_RB = 8;
+    // lumen/ECM relaxation iterations run as regular kernels before the persistent one
+    static constexpr int LUM_REGULAR = 2;
 
     // primaries per block of the column passes (shared tile near 64 KB)
     static constexpr int GB = sizeof(real) == 8 ? 4 : 8;
@@ -1839,7 +2043,7 @@ struct Fused {
         kr_boxD<real, MM, GD><<<dim3((MM / 2 + 1 + GD - 1) / GD, Nt), 256, smD, s>>>(Y1, Y2, ba);
         PFAG_LAUNCHED(c);
         pfag_prof_begin(c, "kf_boxE");
-        kr_boxE<real, MM><<<grow, BG::THREADS, smC, s>>>(Y1, R(c->rho), R(r->Rb), R(c->rhon), c->d_xc, c->d_yc, ba);
+        kr_boxE<real, MM><<<grow, BG::THREADS, smC, s>>>(Y1, R(c->rho), R(r->Rb), c->d_xc, c->d_yc, ba);
         PFAG_LAUNCHED(c);
         return PFAG_OK;
     }

@@ -190,3 +190,33 @@ __device__ __forceinline__ real resh_update(real A, real B,
                     p[2][1] + p[2][0] - p[0][1] - p[0][0], jx_c, jx_jm);
     return pn;
 }
+
+// The same increment for the fused FP32 path with the constants folded:
+// with s = Jn_a + Jn_b, t = Jt_a + Jt_b and h(p) = p (1 - p) a face is
+//   s * ( (A/4)(pa - pb) s + (A/16) tang t - (B/4)(h_a + h_b) ),
+// h is formed once per site of the cross and the tangential differences once
+// per row / column.  FP64 keeps the reference's operation order (resh_update).
+struct ReshConst {
+    float a4, a16, b4;
+};
+__device__ __forceinline__ ReshConst resh_const(double A, double B) {
+    return ReshConst{(float)(A * 0.25), (float)(A * 0.0625), (float)(B * 0.25)};
+}
+__device__ __forceinline__ float resh_face_f(const ReshConst &k, float s, float pa, float pb, float ha, float hb,
+                                             float tang, float t) {
+    return s * fmaf(k.a4 * (pa - pb), s, fmaf(k.a16 * tang, t, -k.b4 * (ha + hb)));
+}
+__device__ __forceinline__ float resh_update_f(const ReshConst &k, const float p[3][3], float jx_c, float jx_ip,
+                                               float jx_im, float jx_jp, float jx_jm, float jy_c, float jy_ip,
+                                               float jy_im, float jy_jp, float jy_jm, float pn) {
+    const float hc = fmaf(-p[1][1], p[1][1], p[1][1]);
+    const float hip = fmaf(-p[2][1], p[2][1], p[2][1]), him = fmaf(-p[0][1], p[0][1], p[0][1]);
+    const float hjp = fmaf(-p[1][2], p[1][2], p[1][2]), hjm = fmaf(-p[1][0], p[1][0], p[1][0]);
+    const float cd0 = p[0][2] - p[0][0], cd1 = p[1][2] - p[1][0], cd2 = p[2][2] - p[2][0];
+    const float rd0 = p[2][0] - p[0][0], rd1 = p[2][1] - p[0][1], rd2 = p[2][2] - p[0][2];
+    pn += resh_face_f(k, jx_ip + jx_c, p[2][1], p[1][1], hip, hc, cd2 + cd1, jy_ip + jy_c);
+    pn += resh_face_f(k, jy_jp + jy_c, p[1][2], p[1][1], hjp, hc, rd2 + rd1, jx_jp + jx_c);
+    pn -= resh_face_f(k, jx_c + jx_im, p[1][1], p[0][1], hc, him, cd1 + cd0, jy_c + jy_im);
+    pn -= resh_face_f(k, jy_c + jy_jm, p[1][1], p[1][0], hc, hjm, rd1 + rd0, jx_c + jx_jm);
+    return pn;
+}

@@ -68,3 +68,21 @@ def test_fused_vs_plain_cfg0_fp64():
     for k in ("phi", "rho", "lum", "ECM"):
         assert rel_linf(a[k], b[k]) <= 1e-9, (k, rel_linf(a[k], b[k]))
     assert rel_linf(a["s"], b["s"]) <= 1e-10
+
+
+def test_fused_cfg1_fp64_and_fp32_vs_plain():
+    """The benchmark workload (1024^2, 64 cells, box 256): fused FP64 against
+    the plain FP64 path over 3 steps (support rectangles wider than a block's
+    columns, graph replay from the second step), and the FP32 fused areas
+    against them."""
+    cfg = CONFIGS["cfg1"]()
+    a = run_gpu(cfg, 3, 64, capi.PATH_FUSED)
+    b = run_gpu(cfg, 3, 64, capi.PATH_PLAIN)
+    assert np.array_equal(a["xc"], b["xc"]) and np.array_equal(a["yc"], b["yc"])
+    assert np.array_equal(a["iters"], b["iters"])
+    for k in ("phi", "rho", "lum", "ECM"):
+        assert rel_linf(a[k], b[k]) <= 1e-9, (k, rel_linf(a[k], b[k]))
+    assert rel_linf(a["s"], b["s"]) <= 1e-10
+    f = run_gpu(cfg, 3, 32, capi.PATH_FUSED)
+    assert np.array_equal(f["xc"], b["xc"])
+    assert rel_linf(f["s"], b["s"]) <= 1e-4
