@@ -2001,7 +2001,7 @@ struct Fused {
     static constexpr int LUM_REGULAR = 2;
 
     // primaries per block of the column passes (shared tile near 64 KB)
-    static constexpr int GB = sizeof(real) == 8 ? 4 : 8;
+    static constexpr int GB = 4;
     static constexpr int GD = 2 * GB;
 
     template <int MM>
