@@ -1075,7 +1075,9 @@ __global__ void __launch_bounds__(256) kf_update_tiled(const real *__restrict__ 
             ja = p[c + N] - p[c - N];
             jb = p[c + 1] - p[c - 1];
         }
-        g = sqrt(c4 * (ja * ja + jb * jb));
+        const real q2 = c4 * (ja * ja + jb * jb);
+        if constexpr (sizeof(real) == 8) g = sqrt(q2);
+        else g = q2;                            // FP32 only tests g > 0 and uses rsqrt(q2)
         const size_t jo = (size_t)rr * W + cc;
         const size_t o = base + (size_t)gi * N + gj;
         const real f = sphi[a][b];
@@ -1091,8 +1093,8 @@ __global__ void __launch_bounds__(256) kf_update_tiled(const real *__restrict__ 
                       sigma * ((srho[a + 1][b] - srho[a - 1][b]) * ja + (srho[a][b + 1] - srho[a][b - 1]) * jb) / g;
             }
         } else {
-            // FP32: constant factors folded, one reciprocal of |grad phi|
-            const real rg = (g > (real)0.0) ? (real)1.0 / g : (real)0.0;
+            // FP32: constant factors folded, one reciprocal square root
+            const real rg = (g > (real)0.0) ? rsqrtf(q2) : (real)0.0;
             Jx[jo] = inv2dx * ja * rg;
             Jy[jo] = inv2dx * jb * rg;
             if (rr < 1 || rr > 2 * z || cc < 1 || cc > 2 * z) { phin[o] = f; continue; }

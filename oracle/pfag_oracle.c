@@ -62,6 +62,7 @@ typedef struct {
     cufftHandle planf, planr;
     int iters_cells_max, iters_cells_sum, iters_lum, iters_ecm;
     int *iters_cell;
+    double *rdev_trace;     /* per cell: the last two rdev values of the latest reshaping loop (diagnostics) */
 } pfo_state;
 
 #define C3(n, i, j) ((size_t)(n) * N * N + (size_t)(i) * N + (size_t)(j))
@@ -98,6 +99,7 @@ pfo_state *pfo_create(const pfo_params *p)
     st->s = zalloc(p->Ntot); st->f0 = zalloc(p->Ntot);
     st->xc = (int *)calloc(p->Ntot, sizeof(int)); st->yc = (int *)calloc(p->Ntot, sizeof(int));
     st->iters_cell = (int *)calloc(p->Ntot, sizeof(int));
+    st->rdev_trace = (double *)calloc(2 * (size_t)p->Ntot, sizeof(double));
     cufftComplex **ff[] = {&st->tf, &st->tfr, &st->frho, &st->freact, &st->fxx, &st->fxy, &st->fyy,
                            &st->fvx, &st->fvy, &st->frvx, &st->frvy};
     for (size_t k = 0; k < sizeof(ff) / sizeof(ff[0]); k++) *ff[k] = (cufftComplex *)calloc(mm, sizeof(cufftComplex));
@@ -116,7 +118,7 @@ void pfo_destroy(pfo_state *st)
     cufftComplex *b[] = {st->tf, st->tfr, st->frho, st->freact, st->fxx, st->fxy, st->fyy, st->fvx, st->fvy,
                          st->frvx, st->frvy};
     for (size_t k = 0; k < sizeof(b) / sizeof(b[0]); k++) free(b[k]);
-    free(st->xc); free(st->yc); free(st->iters_cell);
+    free(st->xc); free(st->yc); free(st->iters_cell); free(st->rdev_trace);
     cufftDestroy(st->planf); cufftDestroy(st->planr);
     free(st);
 }
@@ -510,6 +512,8 @@ int pfo_step(pfo_state *st, int it)
             for (int i = st->xc[n] - z; i < st->xc[n] + z; i++)
                 for (int j = st->yc[n] - z; j < st->yc[n] + z; j++)
                     rdev += (FABS(pn[C2(i, j)] - ph[C2(i, j)])) * q->dx * q->dx / q->N_current;
+            st->rdev_trace[2 * n] = st->rdev_trace[2 * n + 1];
+            st->rdev_trace[2 * n + 1] = (double)rdev;
             if (ri > q->rimax) break;
             ri++;
             cnt++;
@@ -535,5 +539,6 @@ real *pfo_field(pfo_state *st, const char *name)
 }
 int *pfo_centres(pfo_state *st, int which) { return which ? st->yc : st->xc; }
 int *pfo_cell_iters(pfo_state *st) { return st->iters_cell; }
+double *pfo_rdev_trace(pfo_state *st) { return st->rdev_trace; }
 int pfo_iters(pfo_state *st, int which) { return which == 0 ? st->iters_lum : st->iters_ecm; }
 int pfo_real_size(void) { return (int)sizeof(real); }

@@ -53,6 +53,8 @@ class Port:
         L.pfo_cell_iters.restype = vp
         L.pfo_cell_iters.argtypes = [vp]
         L.pfo_iters.argtypes = [vp, ctypes.c_int]
+        L.pfo_rdev_trace.restype = vp
+        L.pfo_rdev_trace.argtypes = [vp]
         p = PfoParams()
         for name, t in _FIELDS:
             setattr(p, name, t(params[name]).value)
@@ -97,6 +99,19 @@ class Port:
                 "lum": self._arr("lum", N * N).reshape(N, N), "ECM": self._arr("ECM", N * N).reshape(N, N),
                 "s": self._arr("s", n), "xc": xc, "yc": yc, "cell_iters": it,
                 "lum_iters": self.lib.pfo_iters(self.h, 0), "ecm_iters": self.lib.pfo_iters(self.h, 1)}
+
+
+    def cell_iters(self) -> np.ndarray:
+        """Reshaping iteration count of every cell in the last step."""
+        n = self.ncells
+        return np.frombuffer((ctypes.c_int * n).from_address(self.lib.pfo_cell_iters(self.h)), np.int32).copy()
+
+    def rdev_trace(self) -> np.ndarray:
+        """(Ntot, 2): the last two rdev values of every cell's reshaping loop in
+        the last step (the one before the exit test and the one that passed it)."""
+        n = self.ncells
+        p = self.lib.pfo_rdev_trace(self.h)
+        return np.frombuffer((ctypes.c_double * (2 * n)).from_address(p), np.float64).reshape(n, 2).copy()
 
 
 def run_port(params: dict, init, nsteps: int, precision: int = 64):
