@@ -153,6 +153,14 @@ def measured_peak_hbm():
 
 
 # ---------------------------------------------------------------------------
+# DRAM bytes (read + write) of one launch, from one ncu capture of the fused
+# FP32 path on cfg1 (profiles/fused_cfg1_f32_top_kernels.md: dram__bytes_read.sum
+# + dram__bytes_write.sum, cold caches).  Reported as roofline.traffic for that
+# workload only.
+NCU_TRAFFIC_CFG1_F32 = {"kf_boxB": 74.5e6, "kf_boxA": 110.5e6, "kf_update": 104.2e6, "kf_boxD": 34.4e6,
+                        "kf_resh_first": 55.8e6}
+
+
 def kernel_bytes(cfg, precision: int, iters: dict) -> dict:
     """Algorithmic bytes per launch of the fused kernels (compulsory traffic:
     each array element the kernel must read or write once)."""
@@ -296,7 +304,10 @@ def run_ours(args, ws, rank, local, dist: Dist):
     total_k_ms = sum(v[0] for v in ktimes.values()) or 1.0
     roofline = {"bound": "hbm", "kernel": top_name, "achieved": round(achieved, 1), "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": None, "share": round(top_ms / total_k_ms, 3),
+                "traffic": (NCU_TRAFFIC_CFG1_F32.get(top_name)
+                            if args.config == "cfg1" and prec == 32 else None),
+                "traffic_source": "ncu capture, profiles/fused_cfg1_f32_top_kernels.md",
+                "share": round(top_ms / total_k_ms, 3),
                 "timing": f"per-launch CUDA events over {nprof} eager profiled steps after the timed region",
                 "per_kernel_ms_per_step": {k: round(v[0] / nprof, 4) for k, v in sorted(ktimes.items())},
                 "per_kernel_gbs": {k: round(kb[k] / (v[0] / max(v[1], 1) * 1e-3) / 1e9, 1)
