@@ -698,8 +698,6 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxA(const 
     cx *scr = tw + M;                                   // [ROWS][M] exchange scratch
     real *xys = (real *)(scr + ROWS * M);               // [ROWS][M] pi_xy, read back by the same thread
     unsigned char *cls = (unsigned char *)(xys + ROWS * M);  // [ROWS][M + 4]: padded against bank conflicts
-    fft_twiddles(tw, M);
-    __syncthreads();
     const int t = threadIdx.x % TT, g = threadIdx.x / TT;
     const int n = blockIdx.y, i0 = blockIdx.x * ROWS, i = i0 + g;
     const int N = a.N;
@@ -708,6 +706,28 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxA(const 
     const int n2 = (n == a.Ntot - 1) ? 0 : n + 1;
     const size_t NN = (size_t)N * N;
     const real *p = phi + (size_t)n * NN;
+    // the block's phi rows with a one-site halo ([ROWS + 2][M + 2], in the FFT
+    // exchange scratch, free until the first transform) and its rho rows (in
+    // xys, each element read and then overwritten by the same thread) are
+    // staged by cp.async, so only lum, ECM and the neighbour cells' phi are
+    // read from global memory in the element loop
+    constexpr int PW = M + 2;
+    real *sphi = reinterpret_cast<real *>(scr);
+    {
+        const real *src = p + (size_t)(bi + i0 - 1) * N + (bj - 1);
+        for (int e = threadIdx.x; e < (ROWS + 2) * PW; e += blockDim.x) {
+            const int r = e / PW, cc = e - r * PW;
+            cp_async_elem(sphi + e, src + (size_t)r * N + cc);
+        }
+        const real *rs = rho + (size_t)n * NN + (size_t)(bi + i0) * N + bj;
+        for (int e = threadIdx.x; e < ROWS * M; e += blockDim.x) {
+            const int r = e / M, cc = e - r * M;
+            cp_async_elem(xys + e, rs + (size_t)r * N + cc);
+        }
+    }
+    fft_twiddles(tw, M);
+    cp_async_wait_all();
+    __syncthreads();
     const real c4 = (real)a.c4, sigma = (real)a.sigma;
     const size_t rowo = ((size_t)n * M + i) * M;
     cx v[E1];
@@ -715,12 +735,13 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxA(const 
     for (int q = 0; q < E1; q++) {
         const int j = RF::in_index(t, q);
         const size_t s = (size_t)(bi + i) * N + (bj + j);
-        const real f = p[s];
-        const real dxp = p[s + N] - p[s - N];
-        const real dyp = p[s + 1] - p[s - 1];
+        const int o = (g + 1) * PW + j + 1;
+        const real f = sphi[o];
+        const real dxp = sphi[o + PW] - sphi[o - PW];
+        const real dyp = sphi[o + 1] - sphi[o - 1];
         const real gg = sqrt(c4 * (dxp * dxp + dyp * dyp));
         const int c = map_class_f<real>(f, lum[s], ecm[s], phi[(size_t)n1 * NN + s], phi[(size_t)n2 * NN + s]);
-        const real rr = rho[(size_t)n * NN + s];
+        const real rr = xys[g * M + j];
         const real at = (real)a.a_tan[c], ao = (real)a.a_ort[c], b = (real)a.bb[c];
         real xx = -at * rr * rr * rr + b * rr * rr * rr * rr;
         real yy = xx, xy = (real)0.0;
@@ -749,6 +770,7 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxA(const 
         v[q].x = xx;
         v[q].y = yy;
     }
+    __syncthreads();    // every group is done with the staged phi before scr becomes exchange space
     RF::template run<false>(v, t, scr + g * M, tw);
 #pragma unroll
     for (int r = 0; r < RF::R2; r++)
