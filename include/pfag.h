@@ -161,6 +161,19 @@ int pfag_fn_copy_back(pfag_ctx *ctx);                          /* run_with_activ
 int pfag_areas_noalloc(const void *hfunc_cell, int precision, int Ntot, int N_s, double dx, double alpha,
                        double s0, double *s, double *f0, void *stream);
 
+/* The initial-condition generator, initialisation_code/prepare_initial_files.cpp:53-117,
+ * on the device (a context created with PFAG_PATH_PLAIN).  make_fields != 0:
+ * first the initial fields of functions/initialisation_functions.cpp:62-160
+ * (ini_phi: Ntot cells on a ring of radius Ntot*0.9*R/dx/pi about the centre,
+ * logistic profiles of width wi; ini_ECM_lumen; ini_rho with rho0, tol;
+ * phin = 0); make_fields == 0: the uploaded state stands for them.  Then the
+ * one-shot shaping: centres, phin <- phi, |grad phi| and normals, the cells'
+ * reshaping loops, rho refitted to the cells (update_rho_to_shape,
+ * cell_phase_functions.cpp:42-62), the lumen/ECM update and reshaping.
+ * pfag_download then returns what the reference saves in snapshot slot 1
+ * (the ini_*.bin files it writes, :139-213). */
+int pfag_generate_initial(pfag_ctx *ctx, double rho0, double tol, int make_fields);
+
 /* saving_out_functions (useful_functions.cpp:66-99): device state -> host
  * snapshot slot; phi_out/rho_out get Ntot*N*N, lum_out/ecm_out N*N elements. */
 int pfag_fn_saving_out_functions(pfag_ctx *ctx, void *phi_out, void *rho_out, void *lum_out, void *ecm_out);

@@ -62,6 +62,7 @@ EXPORTS = [
     "pfag_fn_sum_s_kernels", "pfag_fn_update_all_cortices", "pfag_fn_update_lumen_and_ECM",
     "pfag_fn_reshaping_lumen_or_ECM", "pfag_fn_compute_normal_to_phi", "pfag_fn_update_all_cells",
     "pfag_fn_reshaping_cells", "pfag_fn_copy_back", "pfag_fn_saving_out_functions",
+    "pfag_generate_initial",
 ]
 
 
@@ -97,6 +98,7 @@ def lib() -> ctypes.CDLL:
         L.pfag_stream.restype = vp
         L.pfag_launch_count.argtypes = [vp]
         L.pfag_launch_count.restype = ctypes.c_long
+        L.pfag_generate_initial.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int]
         for name in EXPORTS:
             if name.startswith("pfag_fn_"):
                 f = getattr(L, name)
@@ -235,6 +237,11 @@ class Simulation:
 
     def stream(self) -> int:
         return int(lib().pfag_stream(self.h) or 0)
+
+    def generate_initial(self, rho0: float, tol: float, make_fields: bool = True):
+        """prepare_initial_files.cpp:53-117 on the device (plain-path context):
+        the initial fields (make_fields) and their one-shot shaping."""
+        check(lib().pfag_generate_initial(self.h, float(rho0), float(tol), 1 if make_fields else 0))
 
     def fn(self, name: str, *args):
         """Call one per-function entry point, e.g. fn("find_centres_cells")."""

@@ -376,6 +376,13 @@ extern "C" int pfag_fn_sum_s_kernels(pfag_ctx *c, double *s_host, double *f0_hos
     return pfag_get_areas(c, s_host, f0_host);
 }
 
+extern "C" int pfag_generate_initial(pfag_ctx *c, double rho0, double tol, int make_fields) {
+    PFAG_TRY(need_plain(c));
+    if (!(tol > 0.0) || !(rho0 >= 0.0)) { pfag_set_error("rho0 must be >= 0 and tol > 0"); return PFAG_E_ARG; }
+    PFAG_TRY(pfag_plain_generate(c, rho0, tol, make_fields));
+    return fetch_observables(c);
+}
+
 extern "C" int pfag_fn_saving_out_functions(pfag_ctx *c, void *phi_out, void *rho_out, void *lum_out, void *ecm_out) {
     return pfag_download(c, phi_out, rho_out, lum_out, ecm_out);
 }

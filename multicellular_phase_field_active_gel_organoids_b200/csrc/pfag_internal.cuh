@@ -124,6 +124,7 @@ bool pfag_prof_on(pfag_ctx *ctx);
 int pfag_plain_alloc(pfag_ctx *ctx);
 void pfag_plain_free(pfag_ctx *ctx);
 int pfag_plain_step(pfag_ctx *ctx, int it, bool sync_host);
+int pfag_plain_generate(pfag_ctx *ctx, double rho0, double tol, int make_fields);
 int pfag_fused_alloc(pfag_ctx *ctx);
 void pfag_fused_free(pfag_ctx *ctx);
 int pfag_fused_upload_hook(pfag_ctx *ctx);

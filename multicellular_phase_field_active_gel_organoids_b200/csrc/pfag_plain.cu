@@ -594,6 +594,78 @@ __global__ void k_copy(real *__restrict__ dst, const real *__restrict__ src, siz
 }
 
 // ---------------------------------------------------------------------------
+// ---- initial-condition generator (initialisation_code/prepare_initial_files.cpp:53-117)
+
+// ini_phi (functions/initialisation_functions.cpp:116-160): N_ini cells on a
+// ring of radius rcyst about the grid centre (one cell: at the centre), each a
+// logistic profile 1/(1 + exp((dx r - R0)/wi)).  The float build computes the
+// centre in double and stores it as float, r, the exponent and exp in float.
+template <typename real>
+__global__ void k_ini_phi(real *__restrict__ phi, int N, int N_ini, real dx, real R0, real wi, real rcyst) {
+    const int n = blockIdx.z;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N || j >= N) return;
+    real xcen, ycen;
+    if (N_ini > 1) {
+        xcen = (real)((double)(N / 2) + (double)rcyst * cos((double)n * 2.0 * M_PI / (double)N_ini));
+        ycen = (real)((double)(N / 2) + (double)rcyst * sin((double)n * 2.0 * M_PI / (double)N_ini));
+    } else {
+        xcen = (real)(N / 2);
+        ycen = (real)(N / 2);
+    }
+    const real di = (real)i - xcen, dj = (real)j - ycen;
+    const real e = exp((dx * sqrt(di * di + dj * dj) - R0) / wi);
+    phi[(size_t)n * N * N + (size_t)i * N + j] = (real)(1.0 / (1.0 + (double)e));
+}
+
+// ini_ECM_lumen (initialisation_functions.cpp:72-110): the space the cells
+// leave free, 1 - sum phi, is lumen inside the ring radius and ECM outside;
+// zero where the cells fill the site.  Sites not assigned stay zero.
+template <typename real>
+__global__ void k_ini_lum_ecm(const real *__restrict__ phi, real *__restrict__ lum, real *__restrict__ ecm, int N,
+                              int N_ini, real rcyst) {
+    const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N || j >= N) return;
+    const size_t k = (size_t)i * N + j, NN = (size_t)N * N;
+    real all = (real)0.0;
+    for (int n = 0; n < N_ini; n++) all += phi[(size_t)n * NN + k];
+    real l = (real)0.0, e = (real)0.0;
+    if (1.0 - (double)all > 0.0) {
+        const int a = i - N / 2, b = j - N / 2;
+        const double d = sqrt((double)(a * a + b * b));
+        if (d < (double)rcyst) l = (real)(1.0 - (double)all);
+        else e = (real)(1.0 - (double)all);
+    }
+    lum[k] = l;
+    ecm[k] = e;
+}
+
+// The cortex density of a phase value (initialisation_functions.cpp:62-70 and
+// update_rho_to_shape, cell_phase_functions.cpp:42-62), in double as both
+// builds evaluate it: rho0 exp(-1/(4 h (1 - h) + tol) + 1/(1 + tol)),
+// h = phi^2 (3 - 2 phi), and 0 below the floor rho0 exp(-1/(2 tol) + 1/(1 + tol)).
+// set_everywhere: ini_rho assigns every site; update_rho_to_shape only sites
+// with phi != 0 (then applies the floor to every site).
+template <typename real>
+__global__ void k_rho_shape(const real *__restrict__ phi, real *__restrict__ rho, size_t n, double rho0, double tol,
+                            int set_everywhere) {
+    // rho0 and tol are parameters of the build's precision
+    rho0 = (double)(real)rho0;
+    tol = (double)(real)tol;
+    const double floor_v = rho0 * exp(-1.0 / (2.0 * tol) + 1.0 / (1.0 + tol));
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const real p = phi[k];
+        const double f = (double)p;
+        const double pp = (double)(p * p);     // phi*phi is a product in the build's precision there
+        real r = rho[k];
+        if (set_everywhere || p != (real)0.0)
+            r = (real)(rho0 * exp(-1.0 / (4.0 * f * f * (3.0 - 2.0 * f) * (1.0 - pp * (3.0 - 2.0 * f)) + tol) +
+                                  1.0 / (1.0 + tol)));
+        if ((double)r < floor_v) r = (real)0.0;
+        rho[k] = r;
+    }
+}
+
 template <typename real> struct FFTX;
 template <> struct FFTX<double> {
     static cufftResult exec(cufftHandle p, void *in, void *out, int dir) {
@@ -854,6 +926,45 @@ struct Plain {
         PFAG_TRY(pfag_check_device_error(c));
         return PFAG_OK;
     }
+    // prepare_initial_files.cpp:53-117: the initial fields (when make_fields),
+    // then centres, phin <- phi, |grad phi| and normals, the cells' reshaping,
+    // rho fitted to the reshaped cells, the lumen/ECM update and their
+    // reshaping.  The reference reads hfunc_lum, hfunc_ECM and psi there before
+    // anything writes them (fresh, zero-filled allocations); they are zeroed.
+    int generate(double rho0, double tol, int make_fields) {
+        const int N = c->N, Nt = c->Ntot;
+        cudaStream_t s = c->stream;
+        PFAG_CUDA_CHECK(cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), s));
+        const real rcyst = (real)((double)Nt * 0.9 * c->p.R / c->p.dx / M_PI);
+        if (make_fields) {
+            const dim3 tb(TBX, TBY), gb((N + TBX - 1) / TBX, (N + TBY - 1) / TBY, Nt);
+            PFAG_CUDA_CHECK(cudaMemsetAsync(c->lum, 0, c->ng * c->rsz, s));
+            PFAG_CUDA_CHECK(cudaMemsetAsync(c->ecm, 0, c->ng * c->rsz, s));
+            k_ini_phi<real><<<gb, tb, 0, s>>>(R(c->phi), N, Nt, (real)c->p.dx, (real)c->p.R, (real)c->p.wi, rcyst);
+            PFAG_LAUNCHED(c);
+            k_ini_lum_ecm<real><<<dim3(gb.x, gb.y), tb, 0, s>>>(R(c->phi), R(c->lum), R(c->ecm), N, Nt, rcyst);
+            PFAG_LAUNCHED(c);
+            k_rho_shape<real><<<1184, 256, 0, s>>>(R(c->phi), R(c->rho), c->nc, rho0, tol, 1);
+            PFAG_LAUNCHED(c);
+        }
+        PFAG_CUDA_CHECK(cudaMemsetAsync(c->hfunc, 0, c->nc * c->rsz, s));
+        PFAG_CUDA_CHECK(cudaMemsetAsync(c->psi, 0, c->ng * c->rsz, s));
+        PFAG_CUDA_CHECK(cudaMemsetAsync(c->hlum, 0, c->ng * c->rsz, s));
+        PFAG_CUDA_CHECK(cudaMemsetAsync(c->hecm, 0, c->ng * c->rsz, s));
+        PFAG_TRY(centres());
+        PFAG_TRY(check_zone());
+        k_copy<real><<<1184, 256, 0, s>>>(R(c->phin), R(c->phi), c->nc); PFAG_LAUNCHED(c);
+        PFAG_TRY(norm_grad());
+        PFAG_TRY(normals());
+        PFAG_TRY(reshape_cells());
+        k_rho_shape<real><<<1184, 256, 0, s>>>(R(c->phi), R(c->rho), c->nc, rho0, tol, 0);
+        PFAG_LAUNCHED(c);
+        PFAG_TRY(lum_ecm_update());
+        PFAG_TRY(reshape_lum(0, &c->stats.lum_iters));
+        PFAG_TRY(reshape_lum(1, &c->stats.ecm_iters));
+        PFAG_CUDA_CHECK(cudaStreamSynchronize(s));
+        return pfag_check_device_error(c);
+    }
     int step(int it) {
         (void)it;
         PFAG_TRY(centres());
@@ -913,6 +1024,11 @@ void pfag_plain_free(pfag_ctx *c) {
 
 int pfag_plain_step(pfag_ctx *c, int it, bool) {
     return c->prec == 64 ? Plain<double>(c).step(it) : Plain<float>(c).step(it);
+}
+
+int pfag_plain_generate(pfag_ctx *c, double rho0, double tol, int make_fields) {
+    return c->prec == 64 ? Plain<double>(c).generate(rho0, tol, make_fields)
+                         : Plain<float>(c).generate(rho0, tol, make_fields);
 }
 
 // Per-function entry points (the drop-in layer's targets).

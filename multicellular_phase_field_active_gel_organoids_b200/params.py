@@ -173,6 +173,17 @@ def small_organoid(name="tiny", N=64, radius=8.0, zone_size=17, steps=10, seed=0
     return OrganoidConfig(name, N, np.array(pts), radius, zone_size, seed, steps)
 
 
+def ring_params(N: int = 96, ncells: int = 6, radius: float = 8.0, zone_size: int = 17) -> dict:
+    """Parameter set of the reference's initial-condition program
+    (initialisation_code/prepare_initial_files.cpp): `ncells` cells of radius
+    `radius` (R0 = R) that it places on a ring of radius ncells*0.9*R/dx/pi,
+    in grid units with the same rescaling as the configurations above; two
+    snapshot slots (before and after the shaping)."""
+    return derive({"N_s": N, "N_ini": ncells, "zone_size": zone_size, "dx": 1.0, "dt": 1e-3, "R0": radius,
+                   "wi": math.sqrt(2.0), "s0": math.pi * radius ** 2, "alpha_ECM": 0.002 * 1e-4,
+                   "rdev_threshold": 50000, "Nsteps": 2, "nsaving": 1, "ndisplay": 1 << 30})
+
+
 CONFIGS = {
     "cfg0": lambda: hex_ring_organoid(),
     "cfg1": lambda: jittered_hex_organoid(),

@@ -17,6 +17,9 @@ Compiles, with g++/gcc on the host,
     drop-in libraries (its step functions over the B200 library):
       oracle/_ref/dropin_main_fp32, oracle/_ref/dropin_main_fp64
     the harness of the drop-in test, not a checker.
+  * the reference's initial-condition program
+    (initialisation_code/prepare_initial_files.cpp) with its step files:
+      oracle/_ref/ref_prepare_fp32, oracle/_ref/ref_prepare_fp64
 
 The reference build needs the reference checkout (default /root/reference,
 override with PFAG_REFERENCE_DIR); where it is absent the prebuilt files in
@@ -146,6 +149,52 @@ def _build_dropin_main(ref: str, double: bool) -> None:
               "-Wl,-rpath," + os.path.join(CUDA_HOME, "lib64"), "-lm"])
 
 
+def _build_prepare(ref: str, double: bool) -> None:
+    """The reference's initial-condition program
+    (initialisation_code/prepare_initial_files.cpp) with its step files, built
+    like the reference's main against the CPU cuFFT shim: the oracle of the
+    device generator (pfag_generate_initial)."""
+    tag = "fp64" if double else "fp32"
+    with tempfile.TemporaryDirectory(prefix=f"pfag_prep_{tag}_") as tmp:
+        src_funcs = os.path.join(ref, "functions")
+        src_main = os.path.join(ref, "initialisation_code", "prepare_initial_files.cpp")
+        if double:
+            for name in REF_FUNCS + REF_HEADERS:
+                text = open(os.path.join(src_funcs, name)).read()
+                open(os.path.join(tmp, name), "w").write(re.sub(r"\bfloat\b", "double", text))
+            text = open(src_main).read()
+            open(os.path.join(tmp, "prepare_initial_files.cpp"), "w").write(re.sub(r"\bfloat\b", "double", text))
+            inc = tmp
+            srcs = [os.path.join(tmp, n) for n in REF_FUNCS] + [os.path.join(tmp, "prepare_initial_files.cpp")]
+        else:
+            inc = src_funcs
+            srcs = [os.path.join(src_funcs, n) for n in REF_FUNCS] + [src_main]
+        defs = ["-DPFAG_REF_DOUBLE"] if double else []
+        incs = ["-I", os.path.join(HERE, "shim_include"), "-I", inc]
+        objs = []
+        for src in srcs + [os.path.join(HERE, "ref_params.cpp")]:
+            obj = os.path.join(tmp, os.path.basename(src) + ".o")
+            _run(["g++", *CXXFLAGS, *defs, *incs, "-c", src, "-o", obj])
+            objs.append(obj)
+        shim = os.path.join(tmp, "cufft_shim.o")
+        _run(["gcc", *CFLAGS, *defs, "-I", os.path.join(HERE, "shim_include"), "-c",
+              os.path.join(HERE, "cufft_shim.c"), "-o", shim])
+        _run(["g++", "-o", os.path.join(REF_OUT, f"ref_prepare_{tag}"), *objs, shim, "-lm"])
+
+
+def build_prepare(force: bool = False) -> bool:
+    """Build oracle/_ref/ref_prepare_fp{32,64}; False when the checkout is absent."""
+    ref = reference_dir()
+    if ref is None:
+        return False
+    os.makedirs(REF_OUT, exist_ok=True)
+    for double in (False, True):
+        tag = "fp64" if double else "fp32"
+        if force or not os.path.exists(os.path.join(REF_OUT, f"ref_prepare_{tag}")):
+            _build_prepare(ref, double)
+    return True
+
+
 def build_dropin_main(force: bool = False) -> bool:
     """Build oracle/_ref/dropin_main_fp{32,64}; needs the reference checkout and
     the package's drop-in libraries.  False when the checkout is absent."""
@@ -198,6 +247,7 @@ def main() -> int:
     build_port(force)
     ok = build_reference(force)
     if ok:
+        build_prepare(force)
         build_dropin_main(force)
     print("oracle port built;", "reference built" if ok else "reference checkout absent (prebuilt files kept)")
     return 0

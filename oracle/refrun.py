@@ -180,3 +180,24 @@ def run_main_binary(binary: str, params: dict, init, workdir: str, env: dict | N
         raise RuntimeError(f"{os.path.basename(binary)} exited with {r.returncode}:\n{r.stderr[-3000:]}")
     n, N = int(params["N_ini"]), int(params["N_s"])
     return fileio.read_state_files(workdir, n, N, prec), r.stderr
+
+
+def run_prepare_binary(binary: str, params: dict, workdir: str, timeout: float = 600.0):
+    """Run a build of the reference's initial-condition program
+    (oracle/_ref/ref_prepare_fp{32,64}) in `workdir` with the parameter set
+    `params`; return the state it writes (ini_*.bin: phi, rho, lum, ECM)."""
+    import subprocess
+    import sys
+    sys.path.insert(0, os.path.dirname(HERE))
+    from multicellular_phase_field_active_gel_organoids_b200 import fileio, params as P
+    prec = 64 if binary.endswith("fp64") else 32
+    os.makedirs(os.path.join(workdir, "data_ini_to_plot"), exist_ok=True)
+    pfile = os.path.join(workdir, "params.txt")
+    P.write_param_file(params, pfile)
+    e = dict(os.environ)
+    e["PFAG_REF_PARAMS"] = pfile
+    r = subprocess.run([binary], cwd=workdir, env=e, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"{os.path.basename(binary)} exited with {r.returncode}:\n{r.stderr[-3000:]}")
+    n, N = int(params["N_ini"]), int(params["N_s"])
+    return fileio.read_state_files(workdir, n, N, prec)
