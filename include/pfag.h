@@ -174,6 +174,21 @@ int pfag_areas_noalloc(const void *hfunc_cell, int precision, int Ntot, int N_s,
  * (the ini_*.bin files it writes, :139-213). */
 int pfag_generate_initial(pfag_ctx *ctx, double rho0, double tol, int make_fields);
 
+/* saving_out_functions (useful_functions.cpp:66-99) without stalling the
+ * steps: the state (phi, rho: Ntot*N*N; lum, ecm: N*N elements) is copied into
+ * a device staging area on the context's stream, then into the given host
+ * buffers on a copy stream while later steps run.  Returns a ticket (>= 0) or
+ * an error code (< 0).  Host buffers should be pinned (cudaHostAlloc) and must
+ * stay untouched until pfag_snapshot_wait(ticket) has returned.  The first call
+ * allocates the staging area (2 Ntot N^2 + 2 N^2 reals). */
+long pfag_snapshot_async(pfag_ctx *ctx, void *phi, void *rho, void *lum, void *ecm);
+int pfag_snapshot_wait(pfag_ctx *ctx, long ticket);
+
+/* One N x N table (precision 32 or 64) written in the reference's text layout,
+ * "%.15f\n" per value and a blank line after each row
+ * (run_with_active_gels.cpp:215-229); host only, several threads. */
+int pfag_write_text_snapshot(const void *table, int precision, int N, const char *path);
+
 /* saving_out_functions (useful_functions.cpp:66-99): device state -> host
  * snapshot slot; phi_out/rho_out get Ntot*N*N, lum_out/ecm_out N*N elements. */
 int pfag_fn_saving_out_functions(pfag_ctx *ctx, void *phi_out, void *rho_out, void *lum_out, void *ecm_out);

@@ -77,6 +77,7 @@ static void free_ctx(pfag_ctx *c) {
     pfag_plain_free(c);
     pfag_fused_free(c);
     pfag_prof_free(c);
+    pfag_snapshot_free(c);
     void *bufs[] = {c->phi, c->phin, c->rho, c->rhon, c->lum, c->lumn, c->ecm, c->ecmn, c->hfunc, c->hlum,
                     c->hecm, c->psi, c->d_xc, c->d_yc, c->d_cacc, c->d_s, c->d_f0, c->d_part, c->d_scal,
                     c->d_iflags, c->d_err, c->d_vx, c->d_vy};

@@ -111,11 +111,13 @@ struct pfag_ctx {
     // fused-path resources (opaque, owned by pfag_fused.cu)
     void *fused;
     void *prof;           // per-kernel event timing (pfag_prof.cu)
+    void *snap;           // asynchronous snapshot staging (pfag_snapshot.cu)
 };
 
 void pfag_prof_begin(pfag_ctx *ctx, const char *name);
 void pfag_prof_end(pfag_ctx *ctx);
 void pfag_prof_free(pfag_ctx *ctx);
+void pfag_snapshot_free(pfag_ctx *ctx);
 bool pfag_prof_on(pfag_ctx *ctx);
 
 // Launch accounting helper; closes the profiling bracket of the launch.
