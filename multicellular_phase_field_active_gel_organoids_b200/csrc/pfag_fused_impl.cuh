@@ -33,10 +33,26 @@
 #include <cmath>
 #include <vector>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 
 namespace cg = cooperative_groups;
 
 namespace {
+
+// The dynamic shared-memory limit is an attribute of a kernel function, shared
+// by every context of the process: raise it to the largest size any context
+// needs and never lower it (contexts of different sizes can coexist).
+inline int smem_at_least(const void *fn, size_t bytes) {
+    static std::mutex mu;
+    static std::map<const void *, size_t> cur;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t &c = cur[fn];
+    if (bytes <= c) return PFAG_OK;
+    PFAG_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    c = bytes;
+    return PFAG_OK;
+}
 
 constexpr int FT = 256;           // threads per block of the fused kernels
 constexpr int SBLK = 32;          // blocks per cell of the support-rectangle reductions
@@ -1778,11 +1794,11 @@ struct Fused {
         r->smemE = r->smemC;
         r->smemB = (M + 2 * 2 * (size_t)G * (M + 1)) * cs;
         r->smemD = (M + 2 * (size_t)G * (M + 1)) * cs;
-        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_boxA<real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smemA));
-        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_boxB<real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smemB));
-        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_boxC<real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smemC));
-        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_boxD<real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smemD));
-        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_boxE<real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smemE));
+        PFAG_TRY(smem_at_least((const void *)kf_boxA<real>, r->smemA));
+        PFAG_TRY(smem_at_least((const void *)kf_boxB<real>, r->smemB));
+        PFAG_TRY(smem_at_least((const void *)kf_boxC<real>, r->smemC));
+        PFAG_TRY(smem_at_least((const void *)kf_boxD<real>, r->smemD));
+        PFAG_TRY(smem_at_least((const void *)kf_boxE<real>, r->smemE));
         int dev = 0, nsm = 0, per = 0;
         PFAG_CUDA_CHECK(cudaGetDevice(&dev));
         PFAG_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -1794,10 +1810,8 @@ struct Fused {
         r->resh_tile = (size_t)3 * (RESH_RB + 2) * (2 * c->zone + 2) * sizeof(real);
         r->resh_smem = (size_t)(r->resh_threads / 32) * c->Ntot * sizeof(double) + r->resh_tile;
         if (r->resh_smem > 200 * 1024) { pfag_set_error("too many cells for the reshaping kernel's per-warp sums"); return PFAG_E_UNSUPPORTED; }
-        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_reshape_strips<real, RESH_RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)r->resh_smem));
-        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kf_resh_first<real, RESH_RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)r->resh_tile));
+        PFAG_TRY(smem_at_least((const void *)kf_reshape_strips<real, RESH_RB>, r->resh_smem));
+        PFAG_TRY(smem_at_least((const void *)kf_resh_first<real, RESH_RB>, r->resh_tile));
         PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kf_reshape_strips<real, RESH_RB>,
                                                                        r->resh_threads, r->resh_smem));
         if (per < 1) { pfag_set_error("reshaping kernel cannot be resident with %d threads", r->resh_threads); return PFAG_E_UNSUPPORTED; }
@@ -1808,8 +1822,7 @@ struct Fused {
         r->tpc = (2 * c->zone + RESH_RB - 1) / RESH_RB;
         r->ntl = ((c->N + LRB - 1) / LRB) * ((c->N + FT - 1) / FT);
         r->lum_tile = (size_t)3 * (LRB + 2) * (FT + 2) * sizeof(real);
-        PFAG_CUDA_CHECK(cudaFuncSetAttribute(kl_relax<real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)r->lum_tile));
+        PFAG_TRY(smem_at_least((const void *)kl_relax<real>, r->lum_tile));
         r->npsi = ((c->N + 31) / 32) * ((c->N + 31) / 32);
         return PFAG_OK;
     }
@@ -2040,15 +2053,11 @@ struct Fused {
         const int nsB = 2 * GB, nsD = 2 * GD;
         const size_t smB = (MM + 2 * (size_t)nsB * (MM + 1)) * cs;
         const size_t smD = (MM + (size_t)nsD * (MM + 1)) * cs;
-        static bool configured = false;
-        if (!configured) {
-            PFAG_CUDA_CHECK(cudaFuncSetAttribute(kr_boxA<real, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
-            PFAG_CUDA_CHECK(cudaFuncSetAttribute(kr_boxB<real, MM, GB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
-            PFAG_CUDA_CHECK(cudaFuncSetAttribute(kr_boxC<real, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smC));
-            PFAG_CUDA_CHECK(cudaFuncSetAttribute(kr_boxD<real, MM, GD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smD));
-            PFAG_CUDA_CHECK(cudaFuncSetAttribute(kr_boxE<real, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smC));
-            configured = true;
-        }
+        PFAG_TRY(smem_at_least((const void *)kr_boxA<real, MM>, smA));
+        PFAG_TRY(smem_at_least((const void *)kr_boxB<real, MM, GB>, smB));
+        PFAG_TRY(smem_at_least((const void *)kr_boxC<real, MM>, smC));
+        PFAG_TRY(smem_at_least((const void *)kr_boxD<real, MM, GD>, smD));
+        PFAG_TRY(smem_at_least((const void *)kr_boxE<real, MM>, smC));
         cx *Y1 = (cx *)r->Y1, *Y2 = (cx *)r->Y2;
         const dim3 grow(MM / BG::ROWS, Nt);
         pfag_prof_begin(c, "kf_boxA");
