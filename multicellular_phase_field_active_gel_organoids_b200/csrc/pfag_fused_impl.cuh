@@ -78,6 +78,10 @@ struct FusedRes {
     int ntl;                // lumen/ECM relaxation tiles per field (LRB rows x FT columns)
     size_t lum_tile;        // their staged tile (3 (LRB+2) (FT+2) reals)
     double *part_lt;        // [2][ntl] tile partial sums
+    // side stream of the lumen/ECM kernels and its fork/join events
+    cudaStream_t side;
+    cudaEvent_t ev_psi, ev_boxA, ev_lum;
+    bool fork;
     int npsi;
     int coop_r, coop_l;     // co-resident block counts of the persistent kernels
     int logm, rows_blk, grp_cols;
@@ -1842,6 +1846,10 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_e, sizeof(double) * r->npsi));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_l, sizeof(double) * 2 * r->coop_l));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_lt, sizeof(double) * 2 * r->ntl));
+        PFAG_CUDA_CHECK(cudaStreamCreateWithFlags(&r->side, cudaStreamNonBlocking));
+        PFAG_CUDA_CHECK(cudaEventCreateWithFlags(&r->ev_psi, cudaEventDisableTiming));
+        PFAG_CUDA_CHECK(cudaEventCreateWithFlags(&r->ev_boxA, cudaEventDisableTiming));
+        PFAG_CUDA_CHECK(cudaEventCreateWithFlags(&r->ev_lum, cudaEventDisableTiming));
         PFAG_CUDA_CHECK(cudaMalloc(&r->cK, sizeof(int) * (3 * c->Ntot + 8)));
         r->cdone = r->cK + c->Ntot;
         r->ccnt = r->cK + 2 * c->Ntot;
@@ -1909,6 +1917,42 @@ struct Fused {
         kf_psi<real><<<dim3(tiles, tiles), FT, 0, s>>>(R(c->hfunc), r->rect, Nt, N, R(c->lum), R(c->ecm), R(c->psi),
                                                         R(c->hlum), R(c->hecm), d.dx * d.dx, r->part_e);
         PFAG_LAUNCHED(c);
+        // 6a. lumen / ECM update and normals (cell_phase_functions.cpp:372-444,
+        //     :722-771) need only psi and h(lum), h(ECM): they run on the side
+        //     stream beside the phi update and the spectral solve.  Their
+        //     relaxation (6b) rewrites lum and ECM, so it waits for pass A, which
+        //     reads them.  No cooperative kernel runs beside the side stream: the
+        //     main stream joins it before the persistent kernels.
+        const bool fork = !pfag_prof_on(c);
+        cudaStream_t s2 = fork ? r->side : s;
+        r->fork = fork;
+        if (fork) {
+            PFAG_CUDA_CHECK(cudaEventRecord(r->ev_psi, s));
+            PFAG_CUDA_CHECK(cudaStreamWaitEvent(s2, r->ev_psi, 0));
+        }
+        PFAG_CUDA_CHECK(cudaMemsetAsync(r->lK, 0, sizeof(int) * 8, s2));
+        LumArgs la{};
+        la.N = N; la.rimax = c->p.rimax; la.cap = c->relax_cap; la.npsi = r->npsi;
+        la.dx = d.dx; la.dt = d.dt; la.tau_lum = d.tau_lum; la.xi_lum = d.xi_lum;
+        la.beta_lum_cells = d.beta_lum_cells; la.eta_lum_cells = d.eta_lum_cells; la.beta_lum_ECM = d.beta_lum_ECM;
+        la.alpha_ECM = d.alpha_ECM; la.tau_ECM = d.tau_ECM; la.xi_ECM = d.xi_ECM;
+        la.beta_ECM_cells = d.beta_ECM_cells; la.eta_ECM_cells = d.eta_ECM_cells;
+        la.A = d.A_resh; la.B = d.B_resh; la.thr = d.thr_lum; la.rdev0 = d.rdev0_lum;
+        la.part_e = r->part_e; la.part = r->part_l; la.K = r->lK; la.done = r->ldone; la.cnt = r->lcnt;
+        la.err = c->d_err;
+        {
+            pfag_prof_begin(c, "kfl_sum_ecm");
+            kfl_sum_ecm<<<1, 32, 0, s2>>>(r->part_e, r->npsi, c->d_scal + 0);
+            PFAG_LAUNCHED(c);
+            const dim3 tb(32, 8), gb((N + 31) / 32, (N + 7) / 8);
+            pfag_prof_begin(c, "kfl_update");
+            kfl_update<real><<<gb, tb, 0, s2>>>(R(c->lum), R(c->ecm), R(c->lumn), R(c->ecmn), R(c->psi), R(c->hlum),
+                                                R(c->hecm), c->d_scal + 0, la);
+            PFAG_LAUNCHED(c);
+            pfag_prof_begin(c, "kfl_normals");
+            kfl_normals<real><<<gb, tb, 0, s2>>>(R(c->lum), R(c->lumn), R(c->ecm), R(c->ecmn), R(r->Jl), N, d.dx);
+            PFAG_LAUNCHED(c);
+        }
         // 4. phi update + normals on zone + ring (reads the old rho, like the
         //    spectral solve, which therefore updates rho in place afterwards)
         {
@@ -1934,6 +1978,7 @@ struct Fused {
         kf_boxA<real><<<dim3(M / Rr, Nt), FT, r->smemA, s>>>(R(c->phi), R(c->rho), R(c->lum), R(c->ecm), c->d_xc,
                                                              c->d_yc, ba, Rr, Y1, Y2, R(r->Rb), r->clsT);
         PFAG_LAUNCHED(c);
+        if (r->fork) PFAG_CUDA_CHECK(cudaEventRecord(r->ev_boxA, s));
         const int ngrp = (M / 2 + 1 + G - 1) / G;
         pfag_prof_begin(c, "kf_boxB");
         kf_boxB<real><<<dim3(ngrp, Nt), FT, r->smemB, s>>>(Y1, Y2, r->clsT, ba, G); PFAG_LAUNCHED(c);
@@ -1949,51 +1994,21 @@ struct Fused {
                                                              ba, Rr);
         PFAG_LAUNCHED(c);
         }
-        // 6. lumen / ECM
-        PFAG_CUDA_CHECK(cudaMemsetAsync(r->lK, 0, sizeof(int) * 8, s));
-        {
-            LumArgs la{};
-            la.N = N; la.rimax = c->p.rimax; la.cap = c->relax_cap; la.npsi = r->npsi;
-            la.dx = d.dx; la.dt = d.dt; la.tau_lum = d.tau_lum; la.xi_lum = d.xi_lum;
-            la.beta_lum_cells = d.beta_lum_cells; la.eta_lum_cells = d.eta_lum_cells; la.beta_lum_ECM = d.beta_lum_ECM;
-            la.alpha_ECM = d.alpha_ECM; la.tau_ECM = d.tau_ECM; la.xi_ECM = d.xi_ECM;
-            la.beta_ECM_cells = d.beta_ECM_cells; la.eta_ECM_cells = d.eta_ECM_cells;
-            la.A = d.A_resh; la.B = d.B_resh; la.thr = d.thr_lum; la.rdev0 = d.rdev0_lum;
-            la.part_e = r->part_e; la.part = r->part_l; la.K = r->lK; la.done = r->ldone; la.cnt = r->lcnt;
-            la.err = c->d_err;
-            pfag_prof_begin(c, "kfl_sum_ecm");
-            kfl_sum_ecm<<<1, 32, 0, s>>>(r->part_e, r->npsi, c->d_scal + 0);
+        // 6b. lumen / ECM relaxation: iterations 1 .. LUM_REGULAR as
+        //     full-occupancy kernels on the side stream once pass A has read lum
+        //     and ECM; the rest (if a field still moves) in the persistent kernel
+        //     after the join below
+        if (fork) PFAG_CUDA_CHECK(cudaStreamWaitEvent(s2, r->ev_boxA, 0));
+        for (int it = 1; it <= LUM_REGULAR; it++) {
+            pfag_prof_begin(c, "kl_relax");
+            kl_relax<real><<<dim3(r->ntl, 2), FT, r->lum_tile, s2>>>(R(c->lum), R(c->lumn), R(c->ecm), R(c->ecmn),
+                                                                      R(r->Jl), la, it, r->part_lt);
             PFAG_LAUNCHED(c);
-            const dim3 tb(32, 8), gb((N + 31) / 32, (N + 7) / 8);
-            pfag_prof_begin(c, "kfl_update");
-            kfl_update<real><<<gb, tb, 0, s>>>(R(c->lum), R(c->ecm), R(c->lumn), R(c->ecmn), R(c->psi), R(c->hlum),
-                                               R(c->hecm), c->d_scal + 0, la);
-            PFAG_LAUNCHED(c);
-            pfag_prof_begin(c, "kfl_normals");
-            kfl_normals<real><<<gb, tb, 0, s>>>(R(c->lum), R(c->lumn), R(c->ecm), R(c->ecmn), R(r->Jl), N, d.dx);
-            PFAG_LAUNCHED(c);
-            // iterations 1 .. LUM_REGULAR as full-occupancy kernels, the rest (if
-            // any field is still moving) in the persistent kernel
-            for (int it = 1; it <= LUM_REGULAR; it++) {
-                pfag_prof_begin(c, "kl_relax");
-                kl_relax<real><<<dim3(r->ntl, 2), FT, r->lum_tile, s>>>(R(c->lum), R(c->lumn), R(c->ecm),
-                                                                         R(c->ecmn), R(r->Jl), la, it, r->part_lt);
-                PFAG_LAUNCHED(c);
-                pfag_prof_begin(c, "kl_decide");
-                kl_decide<<<2, 32, 0, s>>>(la, it, r->part_lt, r->ntl);
-                PFAG_LAUNCHED(c);
-            }
-            la.it0 = LUM_REGULAR + 1;
-            real *a0 = R(c->lum), *a1 = R(c->lumn), *a2 = R(c->ecm), *a3 = R(c->ecmn);
-            const real *a4 = R(r->Jl);
-            void *args[] = {&a0, &a1, &a2, &a3, (void *)&a4, &la};
-            pfag_prof_begin(c, "kf_lum");
-            PFAG_TRY(launch_coop_t((const void *)kf_lum<real>, &r->coop_l, FT, args, 0, s));
-            PFAG_LAUNCHED(c);
-            pfag_prof_begin(c, "kl_copy");
-            kl_copy<real><<<dim3(296, 2), FT, 0, s>>>(R(c->lum), R(c->lumn), R(c->ecm), R(c->ecmn), r->lK, N);
+            pfag_prof_begin(c, "kl_decide");
+            kl_decide<<<2, 32, 0, s2>>>(la, it, r->part_lt, r->ntl);
             PFAG_LAUNCHED(c);
         }
+        if (fork) PFAG_CUDA_CHECK(cudaEventRecord(r->ev_lum, s2));
         // 7. reshaping of the cells
         PFAG_CUDA_CHECK(cudaMemsetAsync(r->cK, 0, sizeof(int) * 3 * Nt, s));
         {
@@ -2015,12 +2030,26 @@ struct Fused {
             kf_resh_decide<<<Nt, 32, 0, s>>>(ra, 1);
             PFAG_LAUNCHED(c);
             void *args[] = {&a0, &a1, (void *)&a2, (void *)&a3, (void *)&a4, &ra};
+            if (fork) PFAG_CUDA_CHECK(cudaStreamWaitEvent(s, r->ev_lum, 0));   // join the side stream
             pfag_prof_begin(c, "kf_reshape");
             PFAG_TRY(launch_coop_t((const void *)kf_reshape_strips<real, RESH_RB>, &r->coop_r, r->resh_threads, args,
                                    r->resh_smem, s));
             PFAG_LAUNCHED(c);
             pfag_prof_begin(c, "kf_resh_copy");
             kf_resh_copy<real, RESH_RB><<<gs, r->resh_threads, 0, s>>>(R(c->phi), R(c->phin), c->d_xc, c->d_yc, ra);
+            PFAG_LAUNCHED(c);
+        }
+        // 7b. lumen / ECM iterations beyond LUM_REGULAR, and lum <- lumn, ECM <- ECMn
+        {
+            la.it0 = LUM_REGULAR + 1;
+            real *a0 = R(c->lum), *a1 = R(c->lumn), *a2 = R(c->ecm), *a3 = R(c->ecmn);
+            const real *a4 = R(r->Jl);
+            void *args[] = {&a0, &a1, &a2, &a3, (void *)&a4, &la};
+            pfag_prof_begin(c, "kf_lum");
+            PFAG_TRY(launch_coop_t((const void *)kf_lum<real>, &r->coop_l, FT, args, 0, s));
+            PFAG_LAUNCHED(c);
+            pfag_prof_begin(c, "kl_copy");
+            kl_copy<real><<<dim3(296, 2), FT, 0, s>>>(R(c->lum), R(c->lumn), R(c->ecm), R(c->ecmn), r->lK, N);
             PFAG_LAUNCHED(c);
         }
         // 8. periodic ghost ring of rho
@@ -2064,6 +2093,7 @@ struct Fused {
         kr_boxA<real, MM><<<grow, BG::THREADS, smA, s>>>(R(c->phi), R(c->rho), R(c->lum), R(c->ecm), c->d_xc, c->d_yc,
                                                           ba, Y1, Y2, R(r->Rb), r->clsT);
         PFAG_LAUNCHED(c);
+        if (r->fork) PFAG_CUDA_CHECK(cudaEventRecord(r->ev_boxA, s));
         pfag_prof_begin(c, "kf_boxB");
         kr_boxB<real, MM, GB><<<dim3((MM / 2 + 1 + GB - 1) / GB, Nt), 256, smB, s>>>(Y1, Y2, r->clsT, ba);
         PFAG_LAUNCHED(c);
