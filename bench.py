@@ -187,8 +187,8 @@ def kernel_bytes(cfg, precision: int, iters: dict) -> dict:
         "kf_resh_first": zone * 4 * w,
         # further iterations, per launch
         "kf_reshape": (2 * z) * (2 * z) * 4 * w * (cell_it - n),
-        "kf_psi": N * N * (2 * w + 3 * w) + zone * w,
-        "kf_hfunc_area": zone * 2 * w,
+        # reads phi on the zones (hfunc elsewhere in B_n), lum, ECM; writes hfunc (zones), psi, h(lum), h(ECM)
+        "kf_hpsi": N * N * (2 * w + 3 * w) + zone * 2 * w,
         "kf_centroid": zone * w,
         # read lum, ECM, psi, h(lum), h(ECM); write lumn, ECMn
         "kfl_update": N * N * 7 * w,

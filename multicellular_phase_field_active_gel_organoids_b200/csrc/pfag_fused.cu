@@ -24,7 +24,7 @@ void pfag_fused_free(pfag_ctx *c) {
     cudaEvent_t evs[] = {r->ev_psi, r->ev_boxA, r->ev_lum};
     for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);
     void *bufs[] = {r->Y1, r->Y2, r->Rb, r->clsT, r->Jc, r->Jl, r->rect, r->part_s, r->part_r, r->part_e, r->part_l,
-                    r->part_lt, r->cK};
+                    r->part_lt, r->part_a, r->cK};
     for (void *b : bufs) if (b) cudaFree(b);
     delete r;
     c->fused = nullptr;

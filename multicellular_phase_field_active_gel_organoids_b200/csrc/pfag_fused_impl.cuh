@@ -66,6 +66,7 @@ struct FusedRes {
     void *Jl;               // real [4][N][N] lumen / ECM normals
     int4 *rect;             // [Ntot] support rectangle (i0, i1, j0, j1), half-open
     double *part_s;         // [Ntot][SBLK]
+    double *part_a;         // [Ntot][tiles^2] per-cell area partials of the psi tiles
     double *part_r;         // [Ntot][tpc]
     double *part_e;         // [npsi] sum_ecm partials
     double *part_l;         // [2][coop_l]
@@ -234,75 +235,30 @@ __global__ void kf_centroid_finalize(const long long *__restrict__ acc, int Ntot
     rect[n] = r;
 }
 
-// ---- hfunc on the zone (useful_functions.cpp:233-251) + areas over B_n (:168-190)
+// ---- one pass over 32x32 tiles of the grid: h(phi) on every cell's zone
+//      (compute_hfunc_3d_tables_kernels_loop_n, useful_functions.cpp:233-251),
+//      psi = sum_n hfunc_cell[n] (:305-322), the cells' area partials
+//      (sum_s_kernels, :168-190), h(lum), h(ECM) (:272-285) and the sum_ecm
+//      partials (cell_phase_functions.cpp:376-386).
+// Only the cells whose support rectangle B_n meets the tile are visited, in
+// ascending order (warp 0 compacts them by ballots): hfunc_cell[n] is exactly
+// 0 outside B_n, so psi is the reference's sum in the reference's order.
+// Inside the zone h is formed from phi and stored, elsewhere in B_n the
+// stored (stale) value is read.  Area partials: per cell and tile, the
+// tile's warps' sums in warp order, written to part_a[n][tile].
 template <typename real>
-__global__ void kf_hfunc_area(const real *__restrict__ phi, real *__restrict__ hfunc, const int *__restrict__ xc,
-                              const int *__restrict__ yc, const int4 *__restrict__ rect, int N, int z, double dx2,
-                              double *__restrict__ part) {
-    const int n = blockIdx.y;
-    const int4 r = rect[n];
-    const int zi0 = xc[n] - z, zj0 = yc[n] - z;
-    const size_t base = (size_t)n * N * N;
-    double acc = 0.0;
-    // CR rows x 2 column slots per thread per round, all loads issued first;
-    // inside the zone h is formed from phi and stored, outside it is read
-    constexpr int CR = 4;
-    for (int jb = r.z + threadIdx.x; jb < r.w; jb += 2 * blockDim.x)
-    for (int ib = r.x + blockIdx.x; ib < r.y; ib += CR * gridDim.x) {
-        const int js[2] = {jb, jb + (int)blockDim.x};
-        real v[CR][2];
-        bool inz[CR][2], ok[CR][2];
-#pragma unroll
-        for (int k = 0; k < CR; k++)
-#pragma unroll
-            for (int c = 0; c < 2; c++) {
-                const int i = ib + k * gridDim.x, j = js[c];
-                ok[k][c] = i < r.y && j < r.w;
-                inz[k][c] = i >= zi0 && i < zi0 + 2 * z && j >= zj0 && j < zj0 + 2 * z;
-                v[k][c] = ok[k][c] ? (inz[k][c] ? phi[base + (size_t)i * N + j] : hfunc[base + (size_t)i * N + j])
-                                   : (real)0.0;
-            }
-#pragma unroll
-        for (int k = 0; k < CR; k++)
-#pragma unroll
-            for (int c = 0; c < 2; c++) {
-                if (!ok[k][c]) continue;
-                const int i = ib + k * gridDim.x, j = js[c];
-                real h = v[k][c];
-                if (inz[k][c]) {
-                    h = h * h * ((real)3.0 - (real)2.0 * h);
-                    hfunc[base + (size_t)i * N + j] = h;
-                }
-                acc += (double)h * dx2;
-            }
-    }
-    double s = block_sum_d(acc);
-    if (threadIdx.x == 0) part[(size_t)n * gridDim.x + blockIdx.x] = s;
-}
-
-__global__ void kf_area_finalize(const double *__restrict__ part, int nblk, int Ntot, double alpha, double s0,
-                                 double *__restrict__ s, double *__restrict__ f0) {
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= Ntot) return;
-    double a = 0.0;
-    for (int b = 0; b < nblk; b++) a += part[(size_t)n * nblk + b];
-    s[n] = a;
-    f0[n] = alpha * (s0 - a);
-}
-
-// ---- psi = sum_n hfunc_cell[n] over the cells whose B_n covers the tile,
-//      h(lum), h(ECM) and the sum_ecm partials (useful_functions.cpp:272-322,
-//      cell_phase_functions.cpp:376-386)
-template <typename real>
-__global__ void kf_psi(const real *__restrict__ hfunc, const int4 *__restrict__ rect, int Ntot, int N,
-                       const real *__restrict__ lum, const real *__restrict__ ecm, real *__restrict__ psi,
-                       real *__restrict__ hl, real *__restrict__ he, double dx2, double *__restrict__ part) {
-    // cells whose support rectangle meets this 32x32 tile, in ascending order
-    // (the reference sums n = 0 .. Ntot-1): warp 0 compacts them by ballots
+__global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, real *__restrict__ hfunc,
+                                               const int4 *__restrict__ rect, const int *__restrict__ xc,
+                                               const int *__restrict__ yc, int Ntot, int N, int z,
+                                               const real *__restrict__ lum, const real *__restrict__ ecm,
+                                               real *__restrict__ psi, real *__restrict__ hl, real *__restrict__ he,
+                                               double dx2, double *__restrict__ part_e, double *__restrict__ part_a) {
     __shared__ int list[1024];
     __shared__ int4 lrect[1024];
     __shared__ int nlist;
+    __shared__ double wq[8][32];
     const int ti0 = blockIdx.y * 32, tj0 = blockIdx.x * 32;
+    const int tile = blockIdx.y * gridDim.x + blockIdx.x, ntiles = gridDim.x * gridDim.y;
     if (threadIdx.x < 32) {
         int cnt = 0;
         for (int base = 0; base < Ntot; base += 32) {
@@ -325,37 +281,100 @@ __global__ void kf_psi(const real *__restrict__ hfunc, const int4 *__restrict__ 
     }
     __syncthreads();
     const int nl = nlist;
-    double acc = 0.0;
-    for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
-        const int i = ti0 + (e >> 5), j = tj0 + (e & 31);
-        if (i >= N || j >= N) continue;
-        const size_t s = (size_t)i * N + j;
-        // cells in list order, 8 loads in flight; a cell whose B_n misses the
-        // site contributes an exact 0 (as hfunc_cell does there)
-        real sum = (real)0.0;
-        for (int q0 = 0; q0 < nl; q0 += 8) {
-            real v[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j = tj0 + lane;
+    const size_t NN = (size_t)N * N;
+    real ps[4] = {(real)0.0, (real)0.0, (real)0.0, (real)0.0};
+    for (int q0 = 0; q0 < nl; q0 += 32) {
+        const int qn = min(32, nl - q0);
+        // CU cells per round, all their loads issued before any use
+        constexpr int CU = 4;
+        for (int u0 = 0; u0 < qn; u0 += CU) {
+            real v[CU][4];
+            bool inz[CU][4];
+            real *hp[CU];
 #pragma unroll
-            for (int u = 0; u < 8; u++) {
-                const int q = q0 + u;
-                v[u] = (real)0.0;
-                if (q < nl) {
-                    const int4 r = lrect[q];
-                    if (i >= r.x && i < r.y && j >= r.z && j < r.w) v[u] = hfunc[(size_t)list[q] * N * N + s];
+            for (int c = 0; c < CU; c++) {
+                const int u = u0 + c;
+                const bool live = u < qn;
+                const int q = q0 + (live ? u : 0);
+                const int n = list[q];
+                const int4 r = lrect[q];
+                const int zi0 = xc[n] - z, zj0 = yc[n] - z;
+                hp[c] = hfunc + (size_t)n * NN;
+                const real *pp = phi + (size_t)n * NN;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int i = ti0 + warp + 8 * k;
+                    const bool ok = live && i < N && j < N && i >= r.x && i < r.y && j >= r.z && j < r.w;
+                    inz[c][k] = ok && i >= zi0 && i < zi0 + 2 * z && j >= zj0 && j < zj0 + 2 * z;
+                    const size_t o = (size_t)i * N + j;
+                    v[c][k] = ok ? (inz[c][k] ? pp[o] : hp[c][o]) : (real)0.0;
                 }
             }
 #pragma unroll
-            for (int u = 0; u < 8; u++) sum += v[u];
+            for (int c = 0; c < CU; c++) {
+                double a = 0.0;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    real h = v[c][k];
+                    if (inz[c][k]) {
+                        h = h * h * ((real)3.0 - (real)2.0 * h);
+                        hp[c][(size_t)(ti0 + warp + 8 * k) * N + j] = h;
+                    }
+                    ps[k] += h;                 // cells in list order
+                    a += (double)h * dx2;
+                }
+                for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+                if (lane == 0 && u0 + c < qn) wq[warp][u0 + c] = a;
+            }
         }
-        psi[s] = sum;
-        const real a = lum[s], b = ecm[s];
-        hl[s] = a * a * ((real)3.0 - (real)2.0 * a);
+        __syncthreads();
+        if (threadIdx.x < qn) {
+            double t = 0.0;
+#pragma unroll
+            for (int w = 0; w < 8; w++) t += wq[w][threadIdx.x];
+            part_a[(size_t)list[q0 + threadIdx.x] * ntiles + tile] = t;
+        }
+        __syncthreads();
+    }
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int i = ti0 + warp + 8 * k;
+        if (i >= N || j >= N) continue;
+        const size_t o = (size_t)i * N + j;
+        psi[o] = ps[k];
+        const real a = lum[o], b = ecm[o];
+        hl[o] = a * a * ((real)3.0 - (real)2.0 * a);
         const real hb = b * b * ((real)3.0 - (real)2.0 * b);
-        he[s] = hb;
+        he[o] = hb;
         acc += (double)hb * dx2;
     }
-    double t = block_sum_d(acc);
-    if (threadIdx.x == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = t;
+    const double t = block_sum_d(acc);
+    if (threadIdx.x == 0) part_e[tile] = t;
+}
+
+// areas s_n = sum of cell n's tile partials over the tiles B_n meets, in
+// tile order (one warp per cell, fixed summation tree), and
+// f0_n = alpha (s0 - s_n) (useful_functions.cpp:184-187)
+__global__ void kf_area_tiles(const double *__restrict__ part_a, const int4 *__restrict__ rect, int Ntot,
+                              int tiles_x, int ntiles, double alpha, double s0, double *__restrict__ s,
+                              double *__restrict__ f0) {
+    const int n = blockIdx.x, lane = threadIdx.x;
+    const int4 r = rect[n];
+    const int tr0 = r.x / 32, tr1 = (r.y - 1) / 32, tc0 = r.z / 32, tc1 = (r.w - 1) / 32;
+    const int w = tc1 - tc0 + 1, cnt = (tr1 - tr0 + 1) * w;
+    double a = 0.0;
+    for (int k = lane; k < cnt; k += 32) {
+        const int tr = tr0 + k / w, tc = tc0 + k % w;
+        a += part_a[(size_t)n * ntiles + tr * tiles_x + tc];
+    }
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) {
+        s[n] = a;
+        f0[n] = alpha * (s0 - a);
+    }
 }
 
 // ---- box passes -------------------------------------------------------------
@@ -1842,6 +1861,10 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaMalloc(&r->Jl, 4 * c->ng * rs));
         PFAG_CUDA_CHECK(cudaMalloc(&r->rect, sizeof(int4) * c->Ntot));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_s, sizeof(double) * c->Ntot * SBLK));
+        {
+            const size_t t = (size_t)((c->N + 31) / 32);
+            PFAG_CUDA_CHECK(cudaMalloc(&r->part_a, sizeof(double) * c->Ntot * t * t));
+        }
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_r, sizeof(double) * (size_t)c->Ntot * std::max(r->tpc, r->coop_r)));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_e, sizeof(double) * r->npsi));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_l, sizeof(double) * 2 * r->coop_l));
@@ -1903,19 +1926,15 @@ struct Fused {
         kf_centroid_finalize<<<(Nt + 127) / 128, 128, 0, s>>>(c->d_cacc, Nt, N, z, c->d_xc, c->d_yc, r->rect,
                                                                c->d_err);
         PFAG_LAUNCHED(c);
-        // 2. hfunc on the zones, areas over B_n
-        pfag_prof_begin(c, "kf_hfunc_area");
-        kf_hfunc_area<real><<<dim3(SBLK, Nt), FT, 0, s>>>(R(c->phi), R(c->hfunc), c->d_xc, c->d_yc, r->rect, N, z,
-                                                          d.dx * d.dx, r->part_s);
-        PFAG_LAUNCHED(c);
-        pfag_prof_begin(c, "kf_area_finalize");
-        kf_area_finalize<<<(Nt + 127) / 128, 128, 0, s>>>(r->part_s, SBLK, Nt, d.alpha, d.s0, c->d_s, c->d_f0);
-        PFAG_LAUNCHED(c);
-        // 3. psi, h(lum), h(ECM), sum_ecm partials
+        // 2-3. hfunc on the zones, psi, areas, h(lum), h(ECM), sum_ecm partials
         const int tiles = (N + 31) / 32;
-        pfag_prof_begin(c, "kf_psi");
-        kf_psi<real><<<dim3(tiles, tiles), FT, 0, s>>>(R(c->hfunc), r->rect, Nt, N, R(c->lum), R(c->ecm), R(c->psi),
-                                                        R(c->hlum), R(c->hecm), d.dx * d.dx, r->part_e);
+        pfag_prof_begin(c, "kf_hpsi");
+        kf_hpsi<real><<<dim3(tiles, tiles), FT, 0, s>>>(R(c->phi), R(c->hfunc), r->rect, c->d_xc, c->d_yc, Nt, N, z,
+                                                         R(c->lum), R(c->ecm), R(c->psi), R(c->hlum), R(c->hecm),
+                                                         d.dx * d.dx, r->part_e, r->part_a);
+        PFAG_LAUNCHED(c);
+        pfag_prof_begin(c, "kf_area_tiles");
+        kf_area_tiles<<<Nt, 32, 0, s>>>(r->part_a, r->rect, Nt, tiles, tiles * tiles, d.alpha, d.s0, c->d_s, c->d_f0);
         PFAG_LAUNCHED(c);
         // 6a. lumen / ECM update and normals (cell_phase_functions.cpp:372-444,
         //     :722-771) need only psi and h(lum), h(ECM): they run on the side
