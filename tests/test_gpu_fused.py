@@ -86,3 +86,15 @@ def test_fused_cfg1_fp64_and_fp32_vs_plain():
     f = run_gpu(cfg, 3, 32, capi.PATH_FUSED)
     assert np.array_equal(f["xc"], b["xc"])
     assert rel_linf(f["s"], b["s"]) <= 1e-4
+
+
+def test_fused_small_box_shared_memory_path():
+    """Box size 16 (zone_size 9) goes through the shared-memory radix-4 box
+    passes instead of the register FFTs: fused FP64 against plain FP64."""
+    from multicellular_phase_field_active_gel_organoids_b200.params import small_organoid
+    cfg = small_organoid(zone_size=9)
+    a = run_gpu(cfg, 2, 64, capi.PATH_FUSED)
+    b = run_gpu(cfg, 2, 64, capi.PATH_PLAIN)
+    assert np.array_equal(a["iters"], b["iters"])
+    for k in ("phi", "rho", "lum", "ECM"):
+        assert rel_linf(a[k], b[k]) <= 1e-9, (k, rel_linf(a[k], b[k]))
