@@ -34,6 +34,7 @@
 #include <vector>
 #include <cstdlib>
 #include <map>
+#include <type_traits>
 #include <mutex>
 
 namespace cg = cooperative_groups;
@@ -1697,8 +1698,13 @@ __global__ void kl_copy(real *__restrict__ lum, const real *__restrict__ lumn, r
     real *dst = f ? ecm : lum;
     const real *src = f ? ecmn : lumn;
     const size_t NN = (size_t)N * N;
-    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < NN; k += (size_t)gridDim.x * blockDim.x)
-        dst[k] = src[k];
+    // 16-byte vectors (cudaMalloc'd fields are 256-byte aligned), then the tail
+    typedef typename std::conditional<sizeof(real) == 4, float4, double2>::type vec;
+    constexpr int PER = 16 / sizeof(real);
+    const size_t nv = NN / PER;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t k = tid; k < nv; k += stride) reinterpret_cast<vec *>(dst)[k] = reinterpret_cast<const vec *>(src)[k];
+    for (size_t k = nv * PER + tid; k < NN; k += stride) dst[k] = src[k];
 }
 
 // ---- end of step: the periodic ghost ring of rho (boundary_conditions_cells,
