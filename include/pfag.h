@@ -87,6 +87,13 @@ int pfag_sync(pfag_ctx *ctx);
 
 /* Observables of the last step: s (Ntot doubles, cell areas), xc, yc (Ntot ints). */
 int pfag_get_areas(pfag_ctx *ctx, double *s, double *f0);
+/* The areas s, f0 and centres of the last enqueued step (sum_s_kernels and
+ * find_centres_cells results), copied to the given host buffers in stream
+ * order after it, without waiting: valid after pfag_sync (or any later
+ * synchronising call).  Any pointer may be NULL; pinned buffers make the copy
+ * asynchronous.  With pfag_step_async this streams every step's observables
+ * back without a host round trip per step. */
+int pfag_observables_async(pfag_ctx *ctx, double *s, double *f0, int *xc, int *yc);
 int pfag_get_centres(pfag_ctx *ctx, int *xc, int *yc);
 int pfag_get_stats(pfag_ctx *ctx, pfag_stats *st);
 /* Per-cell reshaping iteration counts of the last step (Ntot ints). */

@@ -62,7 +62,7 @@ EXPORTS = [
     "pfag_fn_sum_s_kernels", "pfag_fn_update_all_cortices", "pfag_fn_update_lumen_and_ECM",
     "pfag_fn_reshaping_lumen_or_ECM", "pfag_fn_compute_normal_to_phi", "pfag_fn_update_all_cells",
     "pfag_fn_reshaping_cells", "pfag_fn_copy_back", "pfag_fn_saving_out_functions",
-    "pfag_generate_initial", "pfag_snapshot_async", "pfag_snapshot_wait", "pfag_write_text_snapshot",
+    "pfag_generate_initial", "pfag_observables_async", "pfag_snapshot_async", "pfag_snapshot_wait", "pfag_write_text_snapshot",
 ]
 
 
@@ -99,6 +99,7 @@ def lib() -> ctypes.CDLL:
         L.pfag_launch_count.argtypes = [vp]
         L.pfag_launch_count.restype = ctypes.c_long
         L.pfag_generate_initial.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        L.pfag_observables_async.argtypes = [vp, vp, vp, vp, vp]
         L.pfag_snapshot_async.argtypes = [vp, vp, vp, vp, vp]
         L.pfag_snapshot_async.restype = ctypes.c_long
         L.pfag_snapshot_wait.argtypes = [vp, ctypes.c_long]

@@ -247,6 +247,15 @@ extern "C" int pfag_sync(pfag_ctx *c) {
     return fetch_observables(c);
 }
 
+extern "C" int pfag_observables_async(pfag_ctx *c, double *s, double *f0, int *xc, int *yc) {
+    if (!c) { pfag_set_error("null ctx"); return PFAG_E_ARG; }
+    if (s) PFAG_CUDA_CHECK(cudaMemcpyAsync(s, c->d_s, sizeof(double) * c->Ntot, cudaMemcpyDeviceToHost, c->stream));
+    if (f0) PFAG_CUDA_CHECK(cudaMemcpyAsync(f0, c->d_f0, sizeof(double) * c->Ntot, cudaMemcpyDeviceToHost, c->stream));
+    if (xc) PFAG_CUDA_CHECK(cudaMemcpyAsync(xc, c->d_xc, sizeof(int) * c->Ntot, cudaMemcpyDeviceToHost, c->stream));
+    if (yc) PFAG_CUDA_CHECK(cudaMemcpyAsync(yc, c->d_yc, sizeof(int) * c->Ntot, cudaMemcpyDeviceToHost, c->stream));
+    return PFAG_OK;
+}
+
 extern "C" int pfag_get_areas(pfag_ctx *c, double *s, double *f0) {
     if (!c) return PFAG_E_ARG;
     if (s) std::memcpy(s, c->h_s, sizeof(double) * c->Ntot);

@@ -98,3 +98,30 @@ def test_fused_small_box_shared_memory_path():
     assert np.array_equal(a["iters"], b["iters"])
     for k in ("phi", "rho", "lum", "ECM"):
         assert rel_linf(a[k], b[k]) <= 1e-9, (k, rel_linf(a[k], b[k]))
+
+
+def test_observables_streamed_per_step():
+    """pfag_observables_async after each pfag_step_async: every step's areas and
+    centres arrive in host rows without a wait per step, equal to what the
+    synchronous per-step calls report."""
+    import ctypes
+    cfg = CONFIGS["tiny"]()
+    n, K = cfg.ncells, 4
+    rows = [np.zeros((K, n), np.float64), np.zeros((K, n), np.float64), np.zeros((K, n), np.int32),
+            np.zeros((K, n), np.int32)]
+    with capi.Simulation(cfg.params(), 64, capi.PATH_FUSED) as sim:
+        sim.upload(*cfg.initial_state())
+        for k in range(K):
+            sim.step_async(k, 1)
+            capi.check(capi.lib().pfag_observables_async(sim.h, *[ctypes.c_void_p(a[k].ctypes.data) for a in rows]))
+        sim.sync()
+        s_last, f0_last = sim.areas()
+    with capi.Simulation(cfg.params(), 64, capi.PATH_FUSED) as ref:
+        ref.upload(*cfg.initial_state())
+        for k in range(K):
+            ref.step(k, 1)
+            s, f0 = ref.areas()
+            xc, yc = ref.centres()
+            assert np.array_equal(rows[0][k], s) and np.array_equal(rows[1][k], f0)
+            assert np.array_equal(rows[2][k], xc) and np.array_equal(rows[3][k], yc)
+    assert np.array_equal(rows[0][-1], s_last) and np.array_equal(rows[1][-1], f0_last)
