@@ -983,6 +983,161 @@ __device__ __forceinline__ void store_cols_fixed(cx *__restrict__ dstg, const cx
     for (int i = i0; i < M; i += STEP) dstg[(size_t)i * M + col] = src[(size_t)sl * S + i];
 }
 
+// ---- the divergence of rho v in two passes instead of three --------------
+// update_fft_rho (rho_functions.cpp:213-251) adds D = -i dt kfac (ir (rho vx)^
+// + jr (rho vy)^) to rho^, and the new rho is Re(IFFT2(.))/M^2.  By linearity
+// and because ir depends on the row wavenumber only (jr on the column one),
+//   Re(IFFT2(-i ir FFT2(Fx)))/M^2 = Re(IFFT_i(-i ir FFT_i(Fx)))/M   (columns)
+//   Re(IFFT2(-i jr FFT2(Fy)))/M^2 = Re(IFFT_j(-i jr FFT_j(Fy)))/M   (rows)
+// with Fx = rho Re(vx), Fy = rho Re(vy) (load_fft_rho_v, :267-284): the
+// transforms along the other direction cancel.  Re() keeps the Hermitian part
+// of the multiplied spectrum, which for these odd multipliers is the spectrum
+// with its Nyquist bin (ir or jr = -M/2, its own partner) set to zero.
+//
+// Pass C2 (rows): the inverse row transform of pass B's output gives vx + i vy;
+// Fx is stored for pass D2, and Fy is differentiated along the row at once,
+// dt kfac Re(IFFT_j(-i jr FFT_j(Fy)))/M stored beside it.  X holds Fx, the
+// row term follows at X + Ntot M^2.
+template <typename real, int M>
+__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxC2(const typename Cplx<real>::type *__restrict__ Y1,
+                                               real *__restrict__ X, const real *__restrict__ rho,
+                                               const int *__restrict__ xc, const int *__restrict__ yc, BoxArgs a,
+                                               real *__restrict__ vdx, real *__restrict__ vdy) {
+    typedef typename Cplx<real>::type cx;
+    typedef RegFFT<cx, M> RF;
+    constexpr int TT = RF::TT, E1 = RF::E1, ROWS = BoxGeom<M>::ROWS;
+    extern __shared__ unsigned char smraw[];
+    cx *tw = (cx *)smraw;
+    cx *scr = tw + M;
+    fft_twiddles(tw, M);
+    __syncthreads();
+    const int t = threadIdx.x % TT, g = threadIdx.x / TT;
+    const int n = blockIdx.y, i = blockIdx.x * ROWS + g;
+    const int N = a.N;
+    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
+    const size_t rowo = ((size_t)n * M + i) * M;
+    real *Fx = X + rowo, *Dy = X + (size_t)a.Ntot * M * M + rowo;
+    cx *sm = scr + g * M;
+    cx v[E1];
+#pragma unroll
+    for (int q = 0; q < E1; q++) v[q] = Y1[rowo + RF::in_index(t, q)];
+    RF::template run<true>(v, t, sm, tw);
+    const real mm = (real)((double)M * (double)M);
+    const real *rh = rho + (size_t)n * N * N + (size_t)(bi + i) * N + bj;
+#pragma unroll
+    for (int r = 0; r < RF::R2; r++)
+#pragma unroll
+        for (int k2 = 0; k2 < TT; k2++) {
+            const int k = RF::out_index(t, r, k2);
+            const cx val = v[r * TT + k2];
+            const real rr = rh[k];
+            Fx[k] = rr * val.x / mm;     // load_fft_rho_v, rho_functions.cpp:279
+            cx fy;
+            fy.x = rr * val.y / mm;
+            fy.y = (real)0.0;
+            if (vdx) { vdx[rowo + k] = val.x / mm; vdy[rowo + k] = val.y / mm; }
+            sm[k] = fy;
+        }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < E1; q++) v[q] = sm[RF::in_index(t, q)];
+    __syncwarp();
+    RF::template run<false>(v, t, sm, tw);
+    // times -i jr, Nyquist bin zero
+#pragma unroll
+    for (int r = 0; r < RF::R2; r++)
+#pragma unroll
+        for (int k2 = 0; k2 < TT; k2++) {
+            const int k = RF::out_index(t, r, k2);
+            const real jr = (real)((k == M / 2) ? 0 : wrapk(k, M));
+            const cx x = v[r * TT + k2];
+            cx y;
+            y.x = jr * x.y;
+            y.y = -jr * x.x;
+            sm[k] = y;
+        }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < E1; q++) v[q] = sm[RF::in_index(t, q)];
+    __syncwarp();
+    RF::template run<true>(v, t, sm, tw);
+    const real dtk = (real)(a.dt * a.kfac), inv_m = (real)(1.0 / (double)M);
+#pragma unroll
+    for (int r = 0; r < RF::R2; r++)
+#pragma unroll
+        for (int k2 = 0; k2 < TT; k2++) Dy[RF::out_index(t, r, k2)] = dtk * (v[r * TT + k2].x * inv_m);
+}
+
+// Pass D2 (columns): two real columns of Fx per complex transform (z = a + i b:
+// the i-derivatives of a and b come back in the real and imaginary parts),
+// then the new rho = rho + dt R + column term + row term, in place.
+template <int M> struct BoxGeomD2 {
+    static constexpr int TT = RegFFT<float2, M>::TT;
+    static constexpr int GROUPS = 256 / TT;
+    static constexpr int COLS = (2 * GROUPS < M) ? 2 * GROUPS : M;   // real columns per block
+    static constexpr int NSQ = COLS / 2;                               // complex sequences per block
+};
+template <typename real, int M>
+__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxD2(const real *__restrict__ X, real *__restrict__ rho,
+                                                const real *__restrict__ Rb, const int *__restrict__ xc,
+                                                const int *__restrict__ yc, BoxArgs a) {
+    typedef typename Cplx<real>::type cx;
+    constexpr int S = M + 1, NSQ = BoxGeomD2<M>::NSQ, COLS = BoxGeomD2<M>::COLS;
+    constexpr int WG = BoxGeom<M>::WG;
+    constexpr int NSP = (NSQ % WG == 0) ? NSQ : ((NSQ + WG - 1) / WG) * WG;   // padded to whole warps
+    extern __shared__ unsigned char smraw[];
+    cx *tw = (cx *)smraw;
+    cx *Z = tw + M;                                   // [NSP][S]
+    fft_twiddles(tw, M);
+    const int n = blockIdx.y, c0 = blockIdx.x * COLS;
+    const int N = a.N;
+    const real *fx = X + (size_t)n * M * M, *dy = X + (size_t)a.Ntot * M * M + (size_t)n * M * M;
+    // load column pairs: element (row i, pair p) -> Z[p][i]
+    for (int e = threadIdx.x; e < NSP * M; e += blockDim.x) {
+        const int i = e / NSP, p = e - i * NSP;
+        cx z;
+        if (p < NSQ) {
+            z.x = fx[(size_t)i * M + c0 + 2 * p];
+            z.y = fx[(size_t)i * M + c0 + 2 * p + 1];
+        } else {
+            z.x = (real)0.0; z.y = (real)0.0;
+        }
+        Z[(size_t)p * S + i] = z;
+    }
+    __syncthreads();
+    columns_fft<cx, M, false>(Z, NSP, tw);
+    __syncthreads();
+    // times -i ir, Nyquist bin zero
+    for (int e = threadIdx.x; e < NSQ * M; e += blockDim.x) {
+        const int p = e / M, k = e - p * M;
+        const real ir = (real)((k == M / 2) ? 0 : wrapk(k, M));
+        const cx x = Z[(size_t)p * S + k];
+        cx y;
+        y.x = ir * x.y;
+        y.y = -ir * x.x;
+        Z[(size_t)p * S + k] = y;
+    }
+    __syncthreads();
+    columns_fft<cx, M, true>(Z, NSP, tw);
+    __syncthreads();
+    const real dtk = (real)(a.dt * a.kfac), inv_m = (real)(1.0 / (double)M), dt = (real)a.dt;
+    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
+    real *rcell = rho + (size_t)n * N * N;
+    const real *rb = Rb + (size_t)n * M * M;
+    for (int e = threadIdx.x; e < NSQ * M; e += blockDim.x) {
+        const int i = e / NSQ, p = e - i * NSQ;
+        const cx w = Z[(size_t)p * S + i];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int cc = c0 + 2 * p + h;
+            const size_t bo = (size_t)i * M + cc;
+            const size_t go = (size_t)(bi + i) * N + bj + cc;
+            const real ti = dtk * ((h ? w.y : w.x) * inv_m);
+            rcell[go] = rcell[go] + dt * rb[bo] + (ti + dy[bo]);
+        }
+    }
+}
+
 template <typename real, int M, int G>
 __global__ void __launch_bounds__(256) kr_boxB(typename Cplx<real>::type *__restrict__ Y1,
                                                const typename Cplx<real>::type *__restrict__ Y2,
@@ -2104,14 +2259,15 @@ struct Fused {
         const size_t smA = (MM + (size_t)BG::ROWS * MM) * cs + (size_t)BG::ROWS * MM * sizeof(real) +
                            (size_t)BG::ROWS * (MM + 4);
         const size_t smC = (MM + (size_t)BG::ROWS * MM) * cs;
-        const int nsB = 2 * GB, nsD = 2 * GD;
+        const int nsB = 2 * GB;
         const size_t smB = (MM + 2 * (size_t)nsB * (MM + 1)) * cs;
-        const size_t smD = (MM + (size_t)nsD * (MM + 1)) * cs;
         PFAG_TRY(smem_at_least((const void *)kr_boxA<real, MM>, smA));
         PFAG_TRY(smem_at_least((const void *)kr_boxB<real, MM, GB>, smB));
-        PFAG_TRY(smem_at_least((const void *)kr_boxC<real, MM>, smC));
-        PFAG_TRY(smem_at_least((const void *)kr_boxD<real, MM, GD>, smD));
-        PFAG_TRY(smem_at_least((const void *)kr_boxE<real, MM>, smC));
+        typedef BoxGeomD2<MM> BD;
+        constexpr int NSP2 = (BD::NSQ % BG::WG == 0) ? BD::NSQ : ((BD::NSQ + BG::WG - 1) / BG::WG) * BG::WG;
+        const size_t smD2 = (MM + (size_t)NSP2 * (MM + 1)) * cs;
+        PFAG_TRY(smem_at_least((const void *)kr_boxC2<real, MM>, smC));
+        PFAG_TRY(smem_at_least((const void *)kr_boxD2<real, MM>, smD2));
         cx *Y1 = (cx *)r->Y1, *Y2 = (cx *)r->Y2;
         const dim3 grow(MM / BG::ROWS, Nt);
         pfag_prof_begin(c, "kf_boxA");
@@ -2122,16 +2278,14 @@ struct Fused {
         pfag_prof_begin(c, "kf_boxB");
         kr_boxB<real, MM, GB><<<dim3((MM / 2 + 1 + GB - 1) / GB, Nt), 256, smB, s>>>(Y1, Y2, r->clsT, ba);
         PFAG_LAUNCHED(c);
+        real *X = (real *)r->Y2;          // pass B is done with Y2: Fx, then the row term
         pfag_prof_begin(c, "kf_boxC");
-        kr_boxC<real, MM><<<grow, BG::THREADS, smC, s>>>(Y1, Y2, R(c->rho), c->d_xc, c->d_yc, ba,
-                                                          c->debug ? R(c->d_vx) : nullptr,
-                                                          c->debug ? R(c->d_vy) : nullptr);
+        kr_boxC2<real, MM><<<grow, BG::THREADS, smC, s>>>(Y1, X, R(c->rho), c->d_xc, c->d_yc, ba,
+                                                           c->debug ? R(c->d_vx) : nullptr,
+                                                           c->debug ? R(c->d_vy) : nullptr);
         PFAG_LAUNCHED(c);
         pfag_prof_begin(c, "kf_boxD");
-        kr_boxD<real, MM, GD><<<dim3((MM / 2 + 1 + GD - 1) / GD, Nt), 256, smD, s>>>(Y1, Y2, ba);
-        PFAG_LAUNCHED(c);
-        pfag_prof_begin(c, "kf_boxE");
-        kr_boxE<real, MM><<<grow, BG::THREADS, smC, s>>>(Y1, R(c->rho), R(r->Rb), c->d_xc, c->d_yc, ba);
+        kr_boxD2<real, MM><<<dim3(MM / BD::COLS, Nt), 256, smD2, s>>>(X, R(c->rho), R(r->Rb), c->d_xc, c->d_yc, ba);
         PFAG_LAUNCHED(c);
         return PFAG_OK;
     }
