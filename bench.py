@@ -177,10 +177,10 @@ def kernel_bytes(cfg, precision: int, iters: dict) -> dict:
         # reads phi (centre), phi_{n-1}, phi_{n+1}, rho, lum, ECM; writes pi_xx+i pi_yy, pi_xy, R, class byte
         "kf_boxA": box * (6 * w + 5 * w + 1),
         "kf_boxB": box * (4 * w + 1 + 2 * w),
+        # reads Y1 (complex), rho; writes Fx and the row term
         "kf_boxC": box * (2 * w + w + 2 * w),
-        "kf_boxD": box * (2 * w + 2 * w),
-        # reads Y1, rho, R; writes rho in place
-        "kf_boxE": box * (2 * w + w + w + w),
+        # reads Fx, the row term, rho, R; writes rho in place
+        "kf_boxD": box * 5 * w,
         # reads phi, rho, hfunc, psi, h(lum), h(ECM); writes phin, J_x, J_y
         "kf_update": ring * 9 * w,
         # reshaping iteration 1: read P and J (x, y), write Q, over every zone

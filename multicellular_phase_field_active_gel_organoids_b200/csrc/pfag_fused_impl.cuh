@@ -834,101 +834,6 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxA(const 
     }
 }
 
-// Pass C on register FFTs.
-template <typename real, int M>
-__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxC(const typename Cplx<real>::type *__restrict__ Y1,
-                                               typename Cplx<real>::type *__restrict__ Y2,
-                                               const real *__restrict__ rho, const int *__restrict__ xc,
-                                               const int *__restrict__ yc, BoxArgs a, real *__restrict__ vdx,
-                                               real *__restrict__ vdy) {
-    typedef typename Cplx<real>::type cx;
-    typedef RegFFT<cx, M> RF;
-    constexpr int TT = RF::TT, E1 = RF::E1, ROWS = BoxGeom<M>::ROWS;
-    extern __shared__ unsigned char smraw[];
-    cx *tw = (cx *)smraw;
-    cx *scr = tw + M;
-    fft_twiddles(tw, M);
-    __syncthreads();
-    const int t = threadIdx.x % TT, g = threadIdx.x / TT;
-    const int n = blockIdx.y, i = blockIdx.x * ROWS + g;
-    const int N = a.N;
-    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
-    const size_t rowo = ((size_t)n * M + i) * M;
-    cx *sm = scr + g * M;
-    cx v[E1];
-#pragma unroll
-    for (int q = 0; q < E1; q++) v[q] = Y1[rowo + RF::in_index(t, q)];
-    RF::template run<true>(v, t, sm, tw);
-    const real mm = (real)((double)M * (double)M);
-    const real *rh = rho + (size_t)n * N * N + (size_t)(bi + i) * N + bj;
-#pragma unroll
-    for (int r = 0; r < RF::R2; r++)
-#pragma unroll
-        for (int k2 = 0; k2 < TT; k2++) {
-            const int k = RF::out_index(t, r, k2);
-            const cx val = v[r * TT + k2];
-            const real rr = rh[k];
-            cx qv;
-            qv.x = rr * val.x / mm;     // load_fft_rho_v, rho_functions.cpp:279
-            qv.y = rr * val.y / mm;
-            if (vdx) { vdx[rowo + k] = val.x / mm; vdy[rowo + k] = val.y / mm; }
-            sm[k] = qv;
-        }
-    __syncwarp();
-#pragma unroll
-    for (int q = 0; q < E1; q++) v[q] = sm[RF::in_index(t, q)];
-    __syncwarp();
-    RF::template run<false>(v, t, sm, tw);
-#pragma unroll
-    for (int r = 0; r < RF::R2; r++)
-#pragma unroll
-        for (int k2 = 0; k2 < TT; k2++) Y2[rowo + RF::out_index(t, r, k2)] = v[r * TT + k2];
-}
-
-// Pass E on register FFTs.
-template <typename real, int M>
-__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxE(const typename Cplx<real>::type *__restrict__ Y1,
-                                               real *__restrict__ rho, const real *__restrict__ Rb,
-                                               const int *__restrict__ xc,
-                                               const int *__restrict__ yc, BoxArgs a) {
-    typedef typename Cplx<real>::type cx;
-    typedef RegFFT<cx, M> RF;
-    constexpr int TT = RF::TT, E1 = RF::E1, ROWS = BoxGeom<M>::ROWS;
-    extern __shared__ unsigned char smraw[];
-    cx *tw = (cx *)smraw;
-    cx *scr = tw + M;
-    fft_twiddles(tw, M);
-    __syncthreads();
-    const int t = threadIdx.x % TT, g = threadIdx.x / TT;
-    const int n = blockIdx.y, i = blockIdx.x * ROWS + g;
-    const int N = a.N;
-    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
-    const size_t rowo = ((size_t)n * M + i) * M;
-    cx v[E1];
-#pragma unroll
-    for (int q = 0; q < E1; q++) v[q] = Y1[rowo + RF::in_index(t, q)];
-    RF::template run<true>(v, t, scr + g * M, tw);
-    const real mm = (real)((double)M * (double)M), dt = (real)a.dt;
-    const size_t so = (size_t)n * N * N + (size_t)(bi + i) * N + bj;
-    // rho is updated in place: all loads of the row segment before the stores
-    real old[E1], rb[E1];
-#pragma unroll
-    for (int r = 0; r < RF::R2; r++)
-#pragma unroll
-        for (int k2 = 0; k2 < TT; k2++) {
-            const int k = RF::out_index(t, r, k2);
-            old[r * TT + k2] = rho[so + k];
-            rb[r * TT + k2] = Rb[rowo + k];
-        }
-#pragma unroll
-    for (int r = 0; r < RF::R2; r++)
-#pragma unroll
-        for (int k2 = 0; k2 < TT; k2++) {
-            const int k = RF::out_index(t, r, k2);
-            rho[so + k] = old[r * TT + k2] + dt * rb[r * TT + k2] + v[r * TT + k2].x / mm;
-        }
-}
-
 // Column transforms of the slots held in shared memory (natural order in and
 // out); each column's own storage is the exchange scratch of its transform.
 template <typename cx, int M, bool INV>
@@ -1190,52 +1095,6 @@ __global__ void __launch_bounds__(256) kr_boxB(typename Cplx<real>::type *__rest
     columns_fft<cx, M, true>(Z1, NSP, tw);
     __syncthreads();
     store_cols_fixed<cx, M, NSP>(Y1 + (size_t)n * M * M, Z1, cs);
-}
-
-template <typename real, int M, int G>
-__global__ void __launch_bounds__(256) kr_boxD(typename Cplx<real>::type *__restrict__ Y1,
-                                               const typename Cplx<real>::type *__restrict__ Y2, BoxArgs a) {
-    typedef typename Cplx<real>::type cx;
-    constexpr int S = M + 1, WG = BoxGeom<M>::WG;
-    extern __shared__ unsigned char smraw[];
-    cx *tw = (cx *)smraw;
-    fft_twiddles(tw, M);
-    __shared__ ColSlots cs;
-    const int n = blockIdx.y;
-    if (threadIdx.x == 0) make_slots(cs, blockIdx.x * G, G, M);
-    __syncthreads();
-    constexpr int NSP = 2 * G;
-    static_assert(NSP % WG == 0, "slot count must be a multiple of the thread groups per warp");
-    cx *W = tw + M;
-    load_cols_fixed<cx, M, NSP>(W, Y2 + (size_t)n * M * M, cs);
-    __syncthreads();
-    columns_fft<cx, M, false>(W, NSP, tw);
-    __syncthreads();
-    const real dtk = (real)(a.dt * a.kfac);
-    for_pairs(cs, M, [&](int sa, int ka, int sb, int kb) {
-        const cx wa = W[(size_t)sa * S + ka], wb = W[(size_t)sb * S + kb];
-        cx A1, B1, A2, B2;
-        A1.x = (real)0.5 * (wa.x + wb.x); A1.y = (real)0.5 * (wa.y - wb.y);
-        B1.x = (real)0.5 * (wa.y + wb.y); B1.y = (real)0.5 * (wb.x - wa.x);
-        A2.x = A1.x; A2.y = -A1.y;
-        B2.x = B1.x; B2.y = -B1.y;
-        const real ir1 = (real)wrapk(ka, M), jr1 = (real)wrapk(cs.col[sa], M);
-        const real ir2 = (real)wrapk(kb, M), jr2 = (real)wrapk(cs.col[sb], M);
-        cx F1, F2, D1, D2;
-        F1.x = ir1 * A1.x + jr1 * B1.x; F1.y = ir1 * A1.y + jr1 * B1.y;
-        F2.x = ir2 * A2.x + jr2 * B2.x; F2.y = ir2 * A2.y + jr2 * B2.y;
-        D1.x = dtk * F1.y; D1.y = -dtk * F1.x;
-        D2.x = dtk * F2.y; D2.y = -dtk * F2.x;
-        cx ha, hb;
-        ha.x = (real)0.5 * (D1.x + D2.x); ha.y = (real)0.5 * (D1.y - D2.y);
-        hb.x = ha.x; hb.y = -ha.y;
-        W[(size_t)sa * S + ka] = ha;
-        if (!(sa == sb && ka == kb)) W[(size_t)sb * S + kb] = hb;
-    });
-    __syncthreads();
-    columns_fft<cx, M, true>(W, NSP, tw);
-    __syncthreads();
-    store_cols_fixed<cx, M, NSP>(Y1 + (size_t)n * M * M, W, cs);
 }
 
 // ---- phi update (cell_phase_functions.cpp:126-217) + normals
@@ -2248,7 +2107,6 @@ struct Fused {
 
     // primaries per block of the column passes (shared tile near 64 KB)
     static constexpr int GB = 4;
-    static constexpr int GD = 2 * GB;
 
     template <int MM>
     int box_reg(const BoxArgs &ba) {
