@@ -1058,16 +1058,23 @@ __global__ void __launch_bounds__(256) kr_boxB(typename Cplx<real>::type *__rest
     __syncthreads();
     constexpr int NSP = 2 * G;               // slots per block (primaries and partners, padded)
     static_assert(NSP % WG == 0, "slot count must be a multiple of the thread groups per warp");
+    // pi_xy is real, so its 2-D spectrum at a pair's partner is the conjugate at
+    // the primary: only the G primary columns of Y2 are transformed
+    constexpr int NZ2 = ((G + WG - 1) / WG) * WG;   // padded to whole warps
+    static_assert((NSP + NZ2) % WG == 0, "slot count must be a multiple of the thread groups per warp");
     cx *Z1 = tw + M, *Z2 = Z1 + (size_t)NSP * S;
     load_cols_fixed<cx, M, NSP>(Z1, Y1 + (size_t)n * M * M, cs);
-    load_cols_fixed<cx, M, NSP>(Z2, Y2 + (size_t)n * M * M, cs);
+    load_cols_fixed<cx, M, NZ2>(Z2, Y2 + (size_t)n * M * M, cs);
     __syncthreads();
-    columns_fft<cx, M, false>(Z1, 2 * NSP, tw);   // Z2 follows Z1 with the same stride
+    columns_fft<cx, M, false>(Z1, NSP + NZ2, tw);   // Z2 follows Z1 with the same stride
     __syncthreads();
     const unsigned char *cl = clsT + (size_t)n * M * M;
     for_pairs(cs, M, [&](int sa, int ka, int sb, int kb) {
         const cx z1a = Z1[(size_t)sa * S + ka], z1b = Z1[(size_t)sb * S + kb];
-        const cx z2a = Z2[(size_t)sa * S + ka], z2b = Z2[(size_t)sb * S + kb];
+        const cx z2a = Z2[(size_t)sa * S + ka];
+        cx z2b;
+        z2b.x = z2a.x;
+        z2b.y = -z2a.y;
         cx pxx_a, pyy_a, pxx_b, pyy_b;
         pxx_a.x = (real)0.5 * (z1a.x + z1b.x); pxx_a.y = (real)0.5 * (z1a.y - z1b.y);
         pyy_a.x = (real)0.5 * (z1a.y + z1b.y); pyy_a.y = (real)0.5 * (z1b.x - z1a.x);
@@ -2118,7 +2125,8 @@ struct Fused {
                            (size_t)BG::ROWS * (MM + 4);
         const size_t smC = (MM + (size_t)BG::ROWS * MM) * cs;
         const int nsB = 2 * GB;
-        const size_t smB = (MM + 2 * (size_t)nsB * (MM + 1)) * cs;
+        const int nz2 = ((GB + BG::WG - 1) / BG::WG) * BG::WG;
+        const size_t smB = (MM + (size_t)(nsB + nz2) * (MM + 1)) * cs;
         PFAG_TRY(smem_at_least((const void *)kr_boxA<real, MM>, smA));
         PFAG_TRY(smem_at_least((const void *)kr_boxB<real, MM, GB>, smB));
         typedef BoxGeomD2<MM> BD;
