@@ -236,7 +236,7 @@ __global__ void kf_centroid_finalize(const long long *__restrict__ acc, int Ntot
     rect[n] = r;
 }
 
-// ---- one pass over 32x32 tiles of the grid: h(phi) on every cell's zone
+// ---- one pass over 16x32 tiles of the grid: h(phi) on every cell's zone
 //      (compute_hfunc_3d_tables_kernels_loop_n, useful_functions.cpp:233-251),
 //      psi = sum_n hfunc_cell[n] (:305-322), the cells' area partials
 //      (sum_s_kernels, :168-190), h(lum), h(ECM) (:272-285) and the sum_ecm
@@ -247,6 +247,7 @@ __global__ void kf_centroid_finalize(const long long *__restrict__ acc, int Ntot
 // Inside the zone h is formed from phi and stored, elsewhere in B_n the
 // stored (stale) value is read.  Area partials: per cell and tile, the
 // tile's warps' sums in warp order, written to part_a[n][tile].
+constexpr int PT_R = 16, KR = PT_R / 8;   // tile rows (tiles are PT_R x 32), rows per thread
 template <typename real>
 __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, real *__restrict__ hfunc,
                                                const int4 *__restrict__ rect, const int *__restrict__ xc,
@@ -258,7 +259,7 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
     __shared__ int4 lrect[1024];
     __shared__ int nlist;
     __shared__ double wq[8][32];
-    const int ti0 = blockIdx.y * 32, tj0 = blockIdx.x * 32;
+    const int ti0 = blockIdx.y * PT_R, tj0 = blockIdx.x * 32;
     const int tile = blockIdx.y * gridDim.x + blockIdx.x, ntiles = gridDim.x * gridDim.y;
     if (threadIdx.x < 32) {
         int cnt = 0;
@@ -268,7 +269,7 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
             bool hit = false;
             if (n < Ntot) {
                 r = rect[n];
-                hit = r.x < ti0 + 32 && r.y > ti0 && r.z < tj0 + 32 && r.w > tj0;
+                hit = r.x < ti0 + PT_R && r.y > ti0 && r.z < tj0 + 32 && r.w > tj0;
             }
             const unsigned m = __ballot_sync(0xffffffffu, hit);
             if (hit) {
@@ -285,14 +286,16 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int j = tj0 + lane;
     const size_t NN = (size_t)N * N;
-    real ps[4] = {(real)0.0, (real)0.0, (real)0.0, (real)0.0};
+    real ps[KR];
+#pragma unroll
+    for (int k = 0; k < KR; k++) ps[k] = (real)0.0;
     for (int q0 = 0; q0 < nl; q0 += 32) {
         const int qn = min(32, nl - q0);
         // CU cells per round, all their loads issued before any use
         constexpr int CU = 4;
         for (int u0 = 0; u0 < qn; u0 += CU) {
-            real v[CU][4];
-            bool inz[CU][4];
+            real v[CU][KR];
+            bool inz[CU][KR];
             real *hp[CU];
 #pragma unroll
             for (int c = 0; c < CU; c++) {
@@ -305,7 +308,7 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
                 hp[c] = hfunc + (size_t)n * NN;
                 const real *pp = phi + (size_t)n * NN;
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
+                for (int k = 0; k < KR; k++) {
                     const int i = ti0 + warp + 8 * k;
                     const bool ok = live && i < N && j < N && i >= r.x && i < r.y && j >= r.z && j < r.w;
                     inz[c][k] = ok && i >= zi0 && i < zi0 + 2 * z && j >= zj0 && j < zj0 + 2 * z;
@@ -317,7 +320,7 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
             for (int c = 0; c < CU; c++) {
                 double a = 0.0;
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
+                for (int k = 0; k < KR; k++) {
                     real h = v[c][k];
                     if (inz[c][k]) {
                         h = h * h * ((real)3.0 - (real)2.0 * h);
@@ -341,7 +344,7 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
     }
     double acc = 0.0;
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
+    for (int k = 0; k < KR; k++) {
         const int i = ti0 + warp + 8 * k;
         if (i >= N || j >= N) continue;
         const size_t o = (size_t)i * N + j;
@@ -364,7 +367,7 @@ __global__ void kf_area_tiles(const double *__restrict__ part_a, const int4 *__r
                               double *__restrict__ f0) {
     const int n = blockIdx.x, lane = threadIdx.x;
     const int4 r = rect[n];
-    const int tr0 = r.x / 32, tr1 = (r.y - 1) / 32, tc0 = r.z / 32, tc1 = (r.w - 1) / 32;
+    const int tr0 = r.x / PT_R, tr1 = (r.y - 1) / PT_R, tc0 = r.z / 32, tc1 = (r.w - 1) / 32;
     const int w = tc1 - tc0 + 1, cnt = (tr1 - tr0 + 1) * w;
     double a = 0.0;
     for (int k = lane; k < cnt; k += 32) {
@@ -1873,7 +1876,7 @@ struct Fused {
         r->ntl = ((c->N + LRB - 1) / LRB) * ((c->N + FT - 1) / FT);
         r->lum_tile = (size_t)3 * (LRB + 2) * (FT + 2) * sizeof(real);
         PFAG_TRY(smem_at_least((const void *)kl_relax<real>, r->lum_tile));
-        r->npsi = ((c->N + 31) / 32) * ((c->N + 31) / 32);
+        r->npsi = ((c->N + 31) / 32) * ((c->N + PT_R - 1) / PT_R);
         return PFAG_OK;
     }
 
@@ -1889,8 +1892,8 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaMalloc(&r->rect, sizeof(int4) * c->Ntot));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_s, sizeof(double) * c->Ntot * SBLK));
         {
-            const size_t t = (size_t)((c->N + 31) / 32);
-            PFAG_CUDA_CHECK(cudaMalloc(&r->part_a, sizeof(double) * c->Ntot * t * t));
+            const size_t t = (size_t)((c->N + 31) / 32) * ((c->N + PT_R - 1) / PT_R);
+            PFAG_CUDA_CHECK(cudaMalloc(&r->part_a, sizeof(double) * c->Ntot * t));
         }
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_r, sizeof(double) * (size_t)c->Ntot * std::max(r->tpc, r->coop_r)));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_e, sizeof(double) * r->npsi));
@@ -1954,14 +1957,15 @@ struct Fused {
                                                                c->d_err);
         PFAG_LAUNCHED(c);
         // 2-3. hfunc on the zones, psi, areas, h(lum), h(ECM), sum_ecm partials
-        const int tiles = (N + 31) / 32;
+        const int tiles = (N + 31) / 32, tiles_r = (N + PT_R - 1) / PT_R;
         pfag_prof_begin(c, "kf_hpsi");
-        kf_hpsi<real><<<dim3(tiles, tiles), FT, 0, s>>>(R(c->phi), R(c->hfunc), r->rect, c->d_xc, c->d_yc, Nt, N, z,
+        kf_hpsi<real><<<dim3(tiles, tiles_r), FT, 0, s>>>(R(c->phi), R(c->hfunc), r->rect, c->d_xc, c->d_yc, Nt, N, z,
                                                          R(c->lum), R(c->ecm), R(c->psi), R(c->hlum), R(c->hecm),
                                                          d.dx * d.dx, r->part_e, r->part_a);
         PFAG_LAUNCHED(c);
         pfag_prof_begin(c, "kf_area_tiles");
-        kf_area_tiles<<<Nt, 32, 0, s>>>(r->part_a, r->rect, Nt, tiles, tiles * tiles, d.alpha, d.s0, c->d_s, c->d_f0);
+        kf_area_tiles<<<Nt, 32, 0, s>>>(r->part_a, r->rect, Nt, tiles, tiles * tiles_r, d.alpha, d.s0, c->d_s,
+                                         c->d_f0);
         PFAG_LAUNCHED(c);
         // 6a. lumen / ECM update and normals (cell_phase_functions.cpp:372-444,
         //     :722-771) need only psi and h(lum), h(ECM): they run on the side
