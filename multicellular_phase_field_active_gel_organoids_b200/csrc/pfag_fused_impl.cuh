@@ -88,6 +88,7 @@ struct FusedRes {
     int coop_r, coop_l;     // co-resident block counts of the persistent kernels
     int logm, rows_blk, grp_cols;
     size_t smemA, smemB, smemC, smemD, smemE;
+    bool ring_pending;      // the rho ghost ring still has to be made to match its sources
     // one step captured as a CUDA graph after the first eager step
     cudaGraph_t graph;
     cudaGraphExec_t gexec;
@@ -209,31 +210,44 @@ __global__ void kf_centroid(const real *__restrict__ phi, const int4 *__restrict
 }
 
 // centroid, zone check (clamped so no kernel can leave the grid), B_n union zone
-__global__ void kf_centroid_finalize(const long long *__restrict__ acc, int Ntot, int N, int zone,
-                                     int *__restrict__ xc, int *__restrict__ yc, int4 *__restrict__ rect,
-                                     unsigned *__restrict__ err) {
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= Ntot) return;
-    long long c = acc[3 * n];
-    int x, y;
+// Cell n's centroid from its accumulators (integer division as the reference,
+// useful_functions.cpp:222-223), clamped so that no kernel can leave the grid,
+// the error bits it raises, and its support rectangle extended by the new zone.
+__device__ __forceinline__ void centroid_of(const long long *__restrict__ acc, int n, int N, int zone, int &x,
+                                            int &y, unsigned &errbits) {
+    const long long c = acc[3 * n];
+    errbits = 0;
     if (c == 0) {
-        atomicOr(err, ERRBIT_EMPTY_CELL);
+        errbits |= ERRBIT_EMPTY_CELL;
         x = N / 2; y = N / 2;
     } else {
         x = (int)(acc[3 * n + 1] / c);
         y = (int)(acc[3 * n + 2] / c);
     }
     if (x - zone < 1 || x + zone > N - 1 || y - zone < 1 || y + zone > N - 1) {
-        atomicOr(err, ERRBIT_ZONE);
+        errbits |= ERRBIT_ZONE;
         x = min(max(x, zone + 1), N - 1 - zone);
         y = min(max(y, zone + 1), N - 1 - zone);
     }
-    xc[n] = x;
-    yc[n] = y;
-    int4 r = rect[n];
+}
+__device__ __forceinline__ int4 rect_with_zone(int4 r, int x, int y, int zone) {
     r.x = min(r.x, x - zone); r.y = max(r.y, x + zone);
     r.z = min(r.z, y - zone); r.w = max(r.w, y + zone);
-    rect[n] = r;
+    return r;
+}
+
+__global__ void kf_centroid_finalize(const long long *__restrict__ acc, int Ntot, int N, int zone,
+                                     int *__restrict__ xc, int *__restrict__ yc, int4 *__restrict__ rect,
+                                     unsigned *__restrict__ err) {
+    int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= Ntot) return;
+    int x, y;
+    unsigned eb;
+    centroid_of(acc, n, N, zone, x, y, eb);
+    if (eb) atomicOr(err, eb);
+    xc[n] = x;
+    yc[n] = y;
+    rect[n] = rect_with_zone(rect[n], x, y, zone);
 }
 
 // ---- one pass over 16x32 tiles of the grid: h(phi) on every cell's zone
@@ -250,13 +264,15 @@ __global__ void kf_centroid_finalize(const long long *__restrict__ acc, int Ntot
 constexpr int PT_R = 16, KR = PT_R / 8;   // tile rows (tiles are PT_R x 32), rows per thread
 template <typename real>
 __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, real *__restrict__ hfunc,
-                                               const int4 *__restrict__ rect, const int *__restrict__ xc,
-                                               const int *__restrict__ yc, int Ntot, int N, int z,
+                                               int4 *__restrict__ rect, const long long *__restrict__ cacc,
+                                               int *__restrict__ xc, int *__restrict__ yc,
+                                               unsigned *__restrict__ err, int Ntot, int N, int z,
                                                const real *__restrict__ lum, const real *__restrict__ ecm,
                                                real *__restrict__ psi, real *__restrict__ hl, real *__restrict__ he,
                                                double dx2, double *__restrict__ part_e, double *__restrict__ part_a) {
     __shared__ int list[1024];
     __shared__ int4 lrect[1024];
+    __shared__ int2 lzone[1024];
     __shared__ int nlist;
     __shared__ double wq[8][32];
     const int ti0 = blockIdx.y * PT_R, tj0 = blockIdx.x * 32;
@@ -266,9 +282,22 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
         for (int base = 0; base < Ntot; base += 32) {
             const int n = base + threadIdx.x;
             int4 r = make_int4(0, 0, 0, 0);
+            int x = 0, y = 0;
             bool hit = false;
             if (n < Ntot) {
-                r = rect[n];
+                // this step's centroid (find_centres_cells) from kf_centroid's sums;
+                // block (0, 0) publishes it for the later kernels, every block
+                // uses its own copy (rect[n] may be old or new here: the union is
+                // the same)
+                unsigned eb;
+                centroid_of(cacc, n, N, z, x, y, eb);
+                r = rect_with_zone(rect[n], x, y, z);
+                if (blockIdx.x == 0 && blockIdx.y == 0) {
+                    if (eb) atomicOr(err, eb);
+                    xc[n] = x;
+                    yc[n] = y;
+                    rect[n] = r;
+                }
                 hit = r.x < ti0 + PT_R && r.y > ti0 && r.z < tj0 + 32 && r.w > tj0;
             }
             const unsigned m = __ballot_sync(0xffffffffu, hit);
@@ -276,6 +305,7 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
                 const int slot = cnt + __popc(m & ((1u << threadIdx.x) - 1u));
                 list[slot] = n;
                 lrect[slot] = r;
+                lzone[slot] = make_int2(x - z, y - z);
             }
             cnt += __popc(m);
         }
@@ -304,7 +334,7 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
                 const int q = q0 + (live ? u : 0);
                 const int n = list[q];
                 const int4 r = lrect[q];
-                const int zi0 = xc[n] - z, zj0 = yc[n] - z;
+                const int zi0 = lzone[q].x, zj0 = lzone[q].y;
                 hp[c] = hfunc + (size_t)n * NN;
                 const real *pp = phi + (size_t)n * NN;
 #pragma unroll
@@ -359,13 +389,12 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
     if (threadIdx.x == 0) part_e[tile] = t;
 }
 
-// areas s_n = sum of cell n's tile partials over the tiles B_n meets, in
-// tile order (one warp per cell, fixed summation tree), and
-// f0_n = alpha (s0 - s_n) (useful_functions.cpp:184-187)
-__global__ void kf_area_tiles(const double *__restrict__ part_a, const int4 *__restrict__ rect, int Ntot,
-                              int tiles_x, int ntiles, double alpha, double s0, double *__restrict__ s,
-                              double *__restrict__ f0) {
-    const int n = blockIdx.x, lane = threadIdx.x;
+// area s_n = sum of cell n's tile partials over the tiles B_n meets, in tile
+// order (lanes take every 32nd tile, then a fixed summation tree): the calling
+// warp returns it on every lane (sum_s_kernels, useful_functions.cpp:168-190)
+__device__ __forceinline__ double cell_area(const double *__restrict__ part_a, const int4 *__restrict__ rect, int n,
+                                            int tiles_x, int ntiles) {
+    const int lane = threadIdx.x & 31;
     const int4 r = rect[n];
     const int tr0 = r.x / PT_R, tr1 = (r.y - 1) / PT_R, tc0 = r.z / 32, tc1 = (r.w - 1) / 32;
     const int w = tc1 - tc0 + 1, cnt = (tr1 - tr0 + 1) * w;
@@ -375,7 +404,14 @@ __global__ void kf_area_tiles(const double *__restrict__ part_a, const int4 *__r
         a += part_a[(size_t)n * ntiles + tr * tiles_x + tc];
     }
     for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if (lane == 0) {
+    return a;
+}
+// s_n and f0_n = alpha (s0 - s_n) (useful_functions.cpp:184-187), one warp per cell
+__global__ void kf_area_tiles(const double *__restrict__ part_a, const int4 *__restrict__ rect, int tiles_x,
+                              int ntiles, double alpha, double s0, double *__restrict__ s, double *__restrict__ f0) {
+    const int n = blockIdx.x;
+    const double a = cell_area(part_a, rect, n, tiles_x, ntiles);
+    if (threadIdx.x == 0) {
         s[n] = a;
         f0[n] = alpha * (s0 - a);
     }
@@ -1940,6 +1976,7 @@ struct Fused {
             pfag_set_error("initial zone leaves the grid or a cell is empty");
             return (c->h_err[0] & ERRBIT_EMPTY_CELL) ? PFAG_E_EMPTY_CELL : PFAG_E_ZONE;
         }
+        r->ring_pending = true;
         return PFAG_OK;
     }
 
@@ -1952,20 +1989,16 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaMemsetAsync(c->d_cacc, 0, sizeof(long long) * 3 * Nt, s));
         pfag_prof_begin(c, "kf_centroid");
         kf_centroid<real><<<dim3(SBLK, Nt), FT, 0, s>>>(R(c->phi), r->rect, N, c->d_cacc); PFAG_LAUNCHED(c);
-        pfag_prof_begin(c, "kf_centroid_finalize");
-        kf_centroid_finalize<<<(Nt + 127) / 128, 128, 0, s>>>(c->d_cacc, Nt, N, z, c->d_xc, c->d_yc, r->rect,
-                                                               c->d_err);
-        PFAG_LAUNCHED(c);
         // 2-3. hfunc on the zones, psi, areas, h(lum), h(ECM), sum_ecm partials
         const int tiles = (N + 31) / 32, tiles_r = (N + PT_R - 1) / PT_R;
         pfag_prof_begin(c, "kf_hpsi");
-        kf_hpsi<real><<<dim3(tiles, tiles_r), FT, 0, s>>>(R(c->phi), R(c->hfunc), r->rect, c->d_xc, c->d_yc, Nt, N, z,
+        kf_hpsi<real><<<dim3(tiles, tiles_r), FT, 0, s>>>(R(c->phi), R(c->hfunc), r->rect, c->d_cacc, c->d_xc,
+                                                           c->d_yc, c->d_err, Nt, N, z,
                                                          R(c->lum), R(c->ecm), R(c->psi), R(c->hlum), R(c->hecm),
                                                          d.dx * d.dx, r->part_e, r->part_a);
         PFAG_LAUNCHED(c);
         pfag_prof_begin(c, "kf_area_tiles");
-        kf_area_tiles<<<Nt, 32, 0, s>>>(r->part_a, r->rect, Nt, tiles, tiles * tiles_r, d.alpha, d.s0, c->d_s,
-                                         c->d_f0);
+        kf_area_tiles<<<Nt, 32, 0, s>>>(r->part_a, r->rect, tiles, tiles * tiles_r, d.alpha, d.s0, c->d_s, c->d_f0);
         PFAG_LAUNCHED(c);
         // 6a. lumen / ECM update and normals (cell_phase_functions.cpp:372-444,
         //     :722-771) need only psi and h(lum), h(ECM): they run on the side
@@ -2102,8 +2135,12 @@ struct Fused {
             kl_copy<real><<<dim3(296, 2), FT, 0, s>>>(R(c->lum), R(c->lumn), R(c->ecm), R(c->ecmn), r->lK, N);
             PFAG_LAUNCHED(c);
         }
-        // 8. periodic ghost ring of rho
-        {
+        // 8. periodic ghost ring of rho (boundary_conditions_cells(rhon),
+        //    rho_functions.cpp:469).  Its sources, rows and columns 1 and N-2,
+        //    lie outside every box (boxes span [xc-z+1, xc+z-2] with
+        //    xc-z >= 1), so once the ring matches them it stays matched: it is
+        //    applied in the first step after an upload only.
+        if (r->ring_pending) {
             pfag_prof_begin(c, "kf_rho_ring");
             kf_rho_ring<real><<<dim3((4 * N + 255) / 256, Nt), 256, 0, s>>>(R(c->rho), N); PFAG_LAUNCHED(c);
         }
@@ -2207,7 +2244,7 @@ template <typename real> int fused_step_t(pfag_ctx *c, bool sync_host) {
         fused_drop_graph(r);
         r->graph_state = 0;
     }
-    if (graphable && r->graph_state == 0 && r->eager_steps >= 1) {
+    if (graphable && r->graph_state == 0 && r->eager_steps >= 1 && !r->ring_pending) {
         cudaStream_t s = c->stream;
         const long l0 = c->launches;
         r->graph_state = -1;
@@ -2229,13 +2266,14 @@ template <typename real> int fused_step_t(pfag_ctx *c, bool sync_host) {
         (void)cudaGetLastError();   // a refused capture leaves a non-sticky error
     }
     int rc = PFAG_OK;
-    if (r->graph_ok) {
+    if (r->graph_ok && !r->ring_pending) {
         PFAG_CUDA_CHECK(cudaGraphLaunch(r->gexec, c->stream));
         c->launches += r->graph_launches;
     } else {
         rc = Fused<real>(c).enqueue();
         if (rc != PFAG_OK) return rc;
         r->eager_steps++;
+        r->ring_pending = false;
     }
     if (sync_host) {
         PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
