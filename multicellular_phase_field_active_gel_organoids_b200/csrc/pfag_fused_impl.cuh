@@ -1036,17 +1036,29 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxD2(const
     const int n = blockIdx.y, c0 = blockIdx.x * COLS;
     const int N = a.N;
     const real *fx = X + (size_t)n * M * M, *dy = X + (size_t)a.Ntot * M * M + (size_t)n * M * M;
-    // load column pairs: element (row i, pair p) -> Z[p][i]
-    for (int e = threadIdx.x; e < NSP * M; e += blockDim.x) {
-        const int i = e / NSP, p = e - i * NSP;
-        cx z;
-        if (p < NSQ) {
-            z.x = fx[(size_t)i * M + c0 + 2 * p];
-            z.y = fx[(size_t)i * M + c0 + 2 * p + 1];
-        } else {
-            z.x = (real)0.0; z.y = (real)0.0;
+    // load column pairs: element (row i, pair p) -> Z[p][i]; U elements per
+    // thread per round, loads first
+    constexpr int U = 4;
+    for (int e0 = threadIdx.x; e0 < NSP * M; e0 += U * blockDim.x) {
+        cx z[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int e = e0 + u * blockDim.x;
+            const int i = e / NSP, p = e - i * NSP;
+            z[u].x = (real)0.0; z[u].y = (real)0.0;
+            if (e < NSP * M && p < NSQ) {
+                z[u].x = fx[(size_t)i * M + c0 + 2 * p];
+                z[u].y = fx[(size_t)i * M + c0 + 2 * p + 1];
+            }
         }
-        Z[(size_t)p * S + i] = z;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int e = e0 + u * blockDim.x;
+            if (e < NSP * M) {
+                const int i = e / NSP, p = e - i * NSP;
+                Z[(size_t)p * S + i] = z[u];
+            }
+        }
     }
     __syncthreads();
     columns_fft<cx, M, false>(Z, NSP, tw);
@@ -1068,16 +1080,36 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxD2(const
     const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
     real *rcell = rho + (size_t)n * N * N;
     const real *rb = Rb + (size_t)n * M * M;
-    for (int e = threadIdx.x; e < NSQ * M; e += blockDim.x) {
-        const int i = e / NSQ, p = e - i * NSQ;
-        const cx w = Z[(size_t)p * S + i];
+    for (int e0 = threadIdx.x; e0 < NSQ * M; e0 += U * blockDim.x) {
+        real ro[U][2], rr[U][2], yy[U][2];
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int cc = c0 + 2 * p + h;
-            const size_t bo = (size_t)i * M + cc;
-            const size_t go = (size_t)(bi + i) * N + bj + cc;
-            const real ti = dtk * ((h ? w.y : w.x) * inv_m);
-            rcell[go] = rcell[go] + dt * rb[bo] + (ti + dy[bo]);
+        for (int u = 0; u < U; u++) {
+            const int e = e0 + u * blockDim.x;
+            if (e < NSQ * M) {
+                const int i = e / NSQ, p = e - i * NSQ;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int cc = c0 + 2 * p + h;
+                    const size_t bo = (size_t)i * M + cc;
+                    ro[u][h] = rcell[(size_t)(bi + i) * N + bj + cc];
+                    rr[u][h] = rb[bo];
+                    yy[u][h] = dy[bo];
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int e = e0 + u * blockDim.x;
+            if (e < NSQ * M) {
+                const int i = e / NSQ, p = e - i * NSQ;
+                const cx w = Z[(size_t)p * S + i];
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int cc = c0 + 2 * p + h;
+                    const real ti = dtk * ((h ? w.y : w.x) * inv_m);
+                    rcell[(size_t)(bi + i) * N + bj + cc] = ro[u][h] + dt * rr[u][h] + (ti + yy[u][h]);
+                }
+            }
         }
     }
 }

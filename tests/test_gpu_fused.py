@@ -125,3 +125,31 @@ def test_observables_streamed_per_step():
             assert np.array_equal(rows[0][k], s) and np.array_equal(rows[1][k], f0)
             assert np.array_equal(rows[2][k], xc) and np.array_equal(rows[3][k], yc)
     assert np.array_equal(rows[0][-1], s_last) and np.array_equal(rows[1][-1], f0_last)
+
+
+def test_rho_ring_after_upload_and_reupload():
+    """The rho ghost ring is made to match its sources in the first step after
+    every upload (its sources never change afterwards): an input whose ring
+    does not match (noise on the ring) must give the plain path's rho, also
+    after a second upload once the step has been captured as a graph."""
+    cfg = CONFIGS["tiny"]()
+    phi, rho, lum, ecm = cfg.initial_state()
+    rng = np.random.default_rng(5)
+    rho = rho.copy()
+    for k in range(rho.shape[0]):
+        rho[k, 0, :] = rng.random(rho.shape[2])
+        rho[k, -1, :] = rng.random(rho.shape[2])
+        rho[k, :, 0] = rng.random(rho.shape[1])
+        rho[k, :, -1] = rng.random(rho.shape[1])
+    out = {}
+    for name, path in (("fused", capi.PATH_FUSED), ("plain", capi.PATH_PLAIN)):
+        with capi.Simulation(cfg.params(), 64, path) as sim:
+            sim.upload(phi, rho, lum, ecm)
+            sim.step(0, 3)
+            first = sim.download()
+            sim.upload(phi, rho, lum, ecm)      # again, after the graph exists
+            sim.step(0, 2)
+            out[name] = (first, sim.download())
+    for a, b in zip(out["fused"], out["plain"]):
+        for x, y in zip(a, b):
+            assert rel_linf(x, y) <= 1e-9
