@@ -181,12 +181,17 @@ def kernel_bytes(cfg, precision: int, iters: dict) -> dict:
         "kf_boxC": box * (2 * w + w + 2 * w),
         # reads Fx, the row term, rho, R; writes rho in place
         "kf_boxD": box * 5 * w,
-        # reads phi, rho, hfunc, psi, h(lum), h(ECM); writes phin, J_x, J_y
-        "kf_update": ring * 9 * w,
-        # reshaping iteration 1: read P and J (x, y), write Q, over every zone
-        "kf_resh_first": zone * 4 * w,
-        # further iterations, per launch
-        "kf_reshape": (2 * z) * (2 * z) * 4 * w * (cell_it - n),
+        # reads phi, rho, hfunc, psi and (FP64) h(lum), h(ECM) or (FP32) the coupling term G;
+        # writes phin, J_x, J_y
+        "kf_update": ring * (9 if precision == 64 else 8) * w,
+        # FP32: reads h(lum), h(ECM), writes G
+        "kf_gel_coupling": N * N * 3 * w,
+        # reshaping iteration 1: read P and J (x, y), write Q and phi (P), over every zone
+        "kf_resh_first": zone * 5 * w,
+        # per launch: further reshaping iterations (read P, J_x, J_y, write Q, phi) and
+        # lumen / ECM iterations beyond the second (read P, J_x, J_y, write Q)
+        "kf_relax_loops": ((2 * z) * (2 * z) * 5 * w * (cell_it - n) +
+                           N * N * 4 * w * (max(lum_it - 2, 0) + max(ecm_it - 2, 0))),
         # reads phi on the zones (hfunc elsewhere in B_n), lum, ECM; writes hfunc (zones), psi, h(lum), h(ECM)
         "kf_hpsi": N * N * (2 * w + 3 * w) + zone * 2 * w,
         "kf_centroid": zone * w,
@@ -196,7 +201,6 @@ def kernel_bytes(cfg, precision: int, iters: dict) -> dict:
         "kfl_normals": N * N * 8 * w,
         # per launch (two launches per step): read P, Jx, Jy, write Q per active field
         "kl_relax": N * N * 4 * w * (min(lum_it, 2) + min(ecm_it, 2)) // 2,
-        "kf_lum": N * N * 4 * w * (max(lum_it - 2, 0) + max(ecm_it - 2, 0)),
     }
     return out
 

@@ -30,6 +30,7 @@
 #include "pfag_regfft.cuh"
 #include <cooperative_groups.h>
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <vector>
 #include <cstdlib>
@@ -70,7 +71,8 @@ struct FusedRes {
     double *part_a;         // [Ntot][tiles^2] per-cell area partials of the psi tiles
     double *part_r;         // [Ntot][tpc]
     double *part_e;         // [npsi] sum_ecm partials
-    double *part_l;         // [2][coop_l]
+    double *part_l;         // [2][coop_r]
+    void *G;                // [N][N] lumen/ECM coupling term of the phi update (FP32 build)
     int *cK, *cdone, *ccnt; // per cell
     int *lK, *ldone, *lcnt; // [2] lumen, ECM
     int tpc;                // reshaping strips per cell
@@ -82,10 +84,10 @@ struct FusedRes {
     double *part_lt;        // [2][ntl] tile partial sums
     // side stream of the lumen/ECM kernels and its fork/join events
     cudaStream_t side;
-    cudaEvent_t ev_psi, ev_boxA, ev_lum;
+    cudaEvent_t ev_psi, ev_area, ev_boxA, ev_lum;
     bool fork;
     int npsi;
-    int coop_r, coop_l;     // co-resident block counts of the persistent kernels
+    int coop_r;             // co-resident block count of the persistent kernel
     int logm, rows_blk, grp_cols;
     size_t smemA, smemB, smemC, smemD, smemE;
     bool ring_pending;      // the rho ghost ring still has to be made to match its sources
@@ -1182,17 +1184,44 @@ __global__ void __launch_bounds__(256) kr_boxB(typename Cplx<real>::type *__rest
 // h(ECM) are staged with a one-site halo, so T is formed once per site and
 // the stencils read shared memory.  Normals on sites whose periodic ghost map
 // is not the identity (a region touching the grid's ghost ring) read their
-// mapped neighbours from global memory.
+// mapped neighbours from global memory.  The FP32 build reads the lumen/ECM
+// coupling term, which is the same for every cell, from G (kf_gel_coupling)
+// and stages only phi, rho and T.
 constexpr int UR = 16, UC = 64;
+
+// The lumen / ECM part of the phi update's bracket (cell_phase_functions.cpp:
+// 126-217): -beta_lum_cells h(lum) + eta_lum_cells lap9(h(lum)) / (4 dx^2)
+// - beta_ECM_cells h(ECM) + eta_ECM_cells lap9(h(ECM)) / (4 dx^2).  No cell
+// enters it, so the FP32 build forms it once per interior site here instead
+// of once per cell and site in kf_update_tiled (rows and columns 0 and N-1,
+// which no zone contains, are left alone).
+template <typename real>
+__global__ void kf_gel_coupling(const real *__restrict__ hl, const real *__restrict__ he, real *__restrict__ G,
+                                DevParams P) {
+    const int N = P.N;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i < 1 || i > N - 2 || j < 1 || j > N - 2) return;
+    const size_t k = (size_t)i * N + j;
+    const real Ll = lap9<real>(hl[k], hl[k + N], hl[k - N], hl[k + 1], hl[k - 1], hl[k + N + 1], hl[k + N - 1],
+                               hl[k - N - 1], hl[k - N + 1]);
+    const real Le = lap9<real>(he[k], he[k + N], he[k - N], he[k + 1], he[k - 1], he[k + N + 1], he[k + N - 1],
+                               he[k - N - 1], he[k - N + 1]);
+    const real iq4 = (real)P.inv_q4;
+    G[k] = -(real)P.beta_lum_cells * hl[k] + (real)P.eta_lum_cells * Ll * iq4 - (real)P.beta_ECM_cells * he[k] +
+           (real)P.eta_ECM_cells * Le * iq4;
+}
+
 template <typename real>
 __global__ void __launch_bounds__(256) kf_update_tiled(const real *__restrict__ phi, real *__restrict__ phin,
                                                        const real *__restrict__ rho, const real *__restrict__ hfunc,
                                                        const double *__restrict__ f0, const real *__restrict__ psi,
                                                        const real *__restrict__ hl, const real *__restrict__ he,
                                                        const int *__restrict__ xc, const int *__restrict__ yc,
-                                                       DevParams P, real *__restrict__ Jc) {
-    constexpr int HR = UR + 2, HC = UC + 2;
-    __shared__ real sphi[HR][HC], srho[HR][HC], sT[HR][HC], shl[HR][HC], she[HR][HC];
+                                                       DevParams P, real *__restrict__ Jc,
+                                                       const real *__restrict__ G) {
+    constexpr bool F32 = sizeof(real) == 4;
+    constexpr int HR = UR + 2, HC = UC + 2, HRg = F32 ? 1 : HR;
+    __shared__ real sphi[HR][HC], srho[HR][HC], sT[HR][HC], shl[HRg][HC], she[HRg][HC];
     const int n = blockIdx.z, N = P.N, z = P.zone, W = 2 * z + 2;
     const int r0 = blockIdx.y * UR, c0 = blockIdx.x * UC;        // region-local tile origin
     const int gi0 = xc[n] - z - 1 + r0, gj0 = yc[n] - z - 1 + c0;  // global origin
@@ -1204,8 +1233,10 @@ __global__ void __launch_bounds__(256) kf_update_tiled(const real *__restrict__ 
         sphi[a][b] = phi[base + k];
         srho[a][b] = rho[base + k];
         sT[a][b] = psi[k] - hfunc[base + k];
-        shl[a][b] = hl[k];
-        she[a][b] = he[k];
+        if constexpr (!F32) {
+            shl[a][b] = hl[k];
+            she[a][b] = he[k];
+        }
     }
     __syncthreads();
     const real dx = (real)P.dx, dt = (real)P.dt, tau = (real)P.tau, sigma = (real)P.sigma;
@@ -1261,11 +1292,11 @@ __global__ void __launch_bounds__(256) kf_update_tiled(const real *__restrict__ 
         const real Tc = sT[a][b];
         const real LT = lap9<real>(Tc, sT[a + 1][b], sT[a - 1][b], sT[a][b + 1], sT[a][b - 1], sT[a + 1][b + 1],
                                    sT[a + 1][b - 1], sT[a - 1][b - 1], sT[a - 1][b + 1]);
-        const real Ll = lap9<real>(shl[a][b], shl[a + 1][b], shl[a - 1][b], shl[a][b + 1], shl[a][b - 1],
-                                   shl[a + 1][b + 1], shl[a + 1][b - 1], shl[a - 1][b - 1], shl[a - 1][b + 1]);
-        const real Le = lap9<real>(she[a][b], she[a + 1][b], she[a - 1][b], she[a][b + 1], she[a][b - 1],
-                                   she[a + 1][b + 1], she[a + 1][b - 1], she[a - 1][b - 1], she[a - 1][b + 1]);
-        if constexpr (sizeof(real) == 8) {
+        if constexpr (!F32) {
+            const real Ll = lap9<real>(shl[a][b], shl[a + 1][b], shl[a - 1][b], shl[a][b + 1], shl[a][b - 1],
+                                       shl[a + 1][b + 1], shl[a + 1][b - 1], shl[a - 1][b - 1], shl[a - 1][b + 1]);
+            const real Le = lap9<real>(she[a][b], she[a + 1][b], she[a - 1][b], she[a][b + 1], she[a][b - 1],
+                                       she[a + 1][b + 1], she[a + 1][b - 1], she[a - 1][b - 1], she[a - 1][b + 1]);
             pn += ((real)1.0 / tau) * f * ((real)1.0 - f) * dt *
                   (fn0 - (real)P.beta * Tc + (real)P.eta * LT / q4 - (real)P.beta_lum_cells * shl[a][b] +
                    (real)P.eta_lum_cells * Ll / q4 - (real)P.beta_ECM_cells * she[a][b] +
@@ -1273,8 +1304,7 @@ __global__ void __launch_bounds__(256) kf_update_tiled(const real *__restrict__ 
         } else {
             const real iq4 = (real)P.inv_q4;
             pn += (real)P.dt_tau * f * ((real)1.0 - f) *
-                  (fn0 - (real)P.beta * Tc + (real)P.eta * LT * iq4 - (real)P.beta_lum_cells * shl[a][b] +
-                   (real)P.eta_lum_cells * Ll * iq4 - (real)P.beta_ECM_cells * she[a][b] + (real)P.eta_ECM_cells * Le * iq4);
+                  (fn0 - (real)P.beta * Tc + (real)P.eta * LT * iq4 + G[(size_t)gi * N + gj]);
         }
         phin[o] = pn;
     }
@@ -1294,11 +1324,18 @@ struct ReshArgs {
 // rows [strip*RB, strip*RB + RB) of Q = P + F(P), one thread per zone column
 // (blockDim >= 2z).  P's strip with its one-row, one-column ring and the
 // normals' strip are staged in shared memory `sm` (3 (RB+2) W reals,
-// W = 2z + 2) and the 3x3 / cross stencils read them there.  Returns this
-// thread's sum of |Q - P| dx^2 / N_current (cell_phase_functions.cpp:554-561).
-// The caller synchronises the block before reusing `sm`.
+// W = 2z + 2) and the 3x3 / cross stencils read them there.  The ring, which
+// no iteration writes, comes from `Pring` (the phi update's output, whose
+// ring holds the old phi); the zone from P.  P's zone values are also stored
+// into `Pout`: the reference keeps the penultimate iterate in phi (the copy
+// phi <- phin at the top of its loop, cell_phase_functions.cpp:470-483), and
+// iteration k's input is iterate k-1, so phi needs no copy after the loop.
+// Returns this thread's sum of |Q - P| dx^2 / N_current
+// (cell_phase_functions.cpp:554-561).  The caller synchronises the block
+// before reusing `sm`.
 template <typename real, int RB>
-__device__ __forceinline__ double resh_tile(const real *__restrict__ P, real *__restrict__ Q,
+__device__ __forceinline__ double resh_tile(const real *__restrict__ P, const real *__restrict__ Pring,
+                                            real *__restrict__ Q, real *__restrict__ Pout,
                                             const real *__restrict__ Jc, const int *__restrict__ xc,
                                             const int *__restrict__ yc, const ReshArgs &a, int n, int strip,
                                             real A, real B, real *sm) {
@@ -1308,13 +1345,17 @@ __device__ __forceinline__ double resh_tile(const real *__restrict__ P, real *__
     const int li0 = strip * RB;
     const int nr = min(RB, Z - li0);
     real *sP = sm, *sX = sm + (RB + 2) * W, *sY = sX + (RB + 2) * W;
-    const real *p = P + (size_t)n * NN + (size_t)(zi0 + li0 - 1) * N + (zj0 - 1);
+    const size_t off = (size_t)n * NN + (size_t)(zi0 + li0 - 1) * N + (zj0 - 1);
+    const real *p = P + off, *pr = Pring + off;
     const real *Jx = Jc + (size_t)n * 2 * W * W + (size_t)li0 * W, *Jy = Jx + (size_t)W * W;
     for (int c = threadIdx.x; c < W; c += blockDim.x) {
+        const bool edge_col = (c == 0 || c == W - 1);
 #pragma unroll
         for (int r = 0; r < RB + 2; r++) {
             if (r < nr + 2) {
-                cp_async_elem(sP + r * W + c, p + (size_t)r * N + c);
+                const int li = li0 + r - 1;                       // zone row; -1 and Z are the ring
+                const bool ring = edge_col || li < 0 || li >= Z;
+                cp_async_elem(sP + r * W + c, (ring ? pr : p) + (size_t)r * N + c);
                 cp_async_elem(sX + r * W + c, Jx + (size_t)r * W + c);
                 cp_async_elem(sY + r * W + c, Jy + (size_t)r * W + c);
             }
@@ -1327,7 +1368,8 @@ __device__ __forceinline__ double resh_tile(const real *__restrict__ P, real *__
     const ReshConst kc = resh_const(a.A, a.B);
     const int j = threadIdx.x;
     if (j < Z) {
-        real *q = Q + (size_t)n * NN + (size_t)(zi0 + li0) * N + zj0 + j;
+        const size_t qo = (size_t)n * NN + (size_t)(zi0 + li0) * N + zj0 + j;
+        real *q = Q + qo, *po = Pout + qo;
         const int c = j + 1;
 #pragma unroll
         for (int r = 0; r < RB; r++) {
@@ -1339,6 +1381,7 @@ __device__ __forceinline__ double resh_tile(const real *__restrict__ P, real *__
 #pragma unroll
                     for (int dj = 0; dj < 3; dj++) w[di][dj] = sP[o + (di - 1) * W + dj - 1];
                 const real old = w[1][1];
+                po[(size_t)r * N] = old;
                 if constexpr (sizeof(real) == 4) {
                     const float nv = resh_update_f(kc, w, sX[o], sX[o + W], sX[o - W], sX[o + 1], sX[o - 1], sY[o],
                                                    sY[o + W], sY[o - W], sY[o + 1], sY[o - 1], old);
@@ -1357,8 +1400,24 @@ __device__ __forceinline__ double resh_tile(const real *__restrict__ P, real *__
     return acc;
 }
 
-// Persistent reshaping of all cells (cell_phase_functions.cpp:461-579) from
-// iteration a.it0 on; a task is one strip of one cell (resh_tile).
+// Loop decision for cell n after iteration `it` (cell_phase_functions.cpp:
+// 554-573) from its summed rdev; lane 0 of the deciding warp calls it.
+__device__ __forceinline__ void resh_decide_cell(const ReshArgs &a, int n, int it, double rdev) {
+    const int k = a.K[n] + 1;
+    a.K[n] = k;
+    bool stop = false;
+    if (k - 1 > a.rimax) { atomicOr(a.err, ERRBIT_RELAX); stop = true; }
+    if (rdev <= a.thr) stop = true;
+    if (!stop && it == a.cap) { atomicOr(a.err, ERRBIT_ITER_CAP); stop = true; }
+    if (stop) a.done[n] = it;
+}
+
+// Persistent reshaping of all cells (cell_phase_functions.cpp:461-579): the
+// decision after iteration 1 (run by kf_resh_first; its per-strip partials
+// part[n][tpc]), then iterations 2.. while a cell still moves; a task is one
+// strip of one cell (resh_tile).  Iterate 0 is phin (the phi update's
+// output), iterate 1 went to T; odd iterations read phin and write T, even
+// ones read T and write phin, and every iteration stores its input into phi.
 // rdev: each warp adds its tasks' sums into its own shared slot per cell (its
 // tasks in a fixed order), the block writes per-cell partials, and after a
 // grid barrier one warp per cell sums the blocks' partials in block order and
@@ -1367,27 +1426,33 @@ __device__ __forceinline__ double resh_tile(const real *__restrict__ P, real *__
 // agrees on the iteration count.
 constexpr int RESH_MAX_THREADS = 384;
 template <typename real, int RB>
-__global__ void __launch_bounds__(RESH_MAX_THREADS) kf_reshape_strips(real *__restrict__ phi, real *__restrict__ phin, const real *__restrict__ Jc,
-                                  const int *__restrict__ xc, const int *__restrict__ yc, ReshArgs a) {
-    cg::grid_group grid = cg::this_grid();
-    extern __shared__ double wacc[];          // [warps][Ntot], then the strip tile
+__device__ __forceinline__ void resh_loops(real *__restrict__ phi, real *__restrict__ phin, real *__restrict__ T,
+                                           const real *__restrict__ Jc, const int *__restrict__ xc,
+                                           const int *__restrict__ yc, const ReshArgs &a, double *wacc,
+                                           cg::grid_group &grid) {
     const real A = (real)a.A, B = (real)a.B;
     const int strips = a.tpc;
     const int total = a.Ntot * strips;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     real *tile = reinterpret_cast<real *>(wacc + nw * a.Ntot);
-    // iterations before it0 ran as separate kernels: nothing left to do?
+    if (warp == 0) {
+        for (int n = blockIdx.x; n < a.Ntot; n += gridDim.x) {
+            const double rdev = warp_sum_fixed(a.part + (size_t)n * strips, strips);
+            if (lane == 0) resh_decide_cell(a, n, a.it0 - 1, rdev);
+        }
+    }
+    grid.sync();
     if (all_done_upto(a.done, a.Ntot, a.it0 - 1)) return;
     for (int it = a.it0; it <= a.cap; it++) {
-        real *P = (it & 1) ? phin : phi;
-        real *Q = (it & 1) ? phi : phin;
+        const real *P = (it & 1) ? phin : T;
+        real *Q = (it & 1) ? T : phin;
         for (int k = threadIdx.x; k < nw * a.Ntot; k += blockDim.x) wacc[k] = 0.0;
         __syncthreads();
         for (int t = blockIdx.x; t < total; t += gridDim.x) {
             const int n = t / strips, strip = t - n * strips;
             const int d = *(volatile int *)&a.done[n];   // not written during this phase
             if (d != 0 && d < it) continue;
-            double acc = resh_tile<real, RB>(P, Q, Jc, xc, yc, a, n, strip, A, B, tile);
+            double acc = resh_tile<real, RB>(P, phin, Q, phi, Jc, xc, yc, a, n, strip, A, B, tile);
             for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
             if (lane == 0) wacc[warp * a.Ntot + n] += acc;
             __syncthreads();
@@ -1403,15 +1468,7 @@ __global__ void __launch_bounds__(RESH_MAX_THREADS) kf_reshape_strips(real *__re
                 const int d = *(volatile int *)&a.done[n];
                 if (d != 0 && d < it) continue;
                 const double rdev = warp_sum_fixed(a.part + (size_t)n * gridDim.x, (int)gridDim.x);
-                if (lane == 0) {
-                    const int done_iters = a.K[n] + 1;
-                    a.K[n] = done_iters;
-                    bool stop = false;
-                    if (done_iters - 1 > a.rimax) { atomicOr(a.err, ERRBIT_RELAX); stop = true; }
-                    if (rdev <= a.thr) stop = true;
-                    if (!stop && it == a.cap) { atomicOr(a.err, ERRBIT_ITER_CAP); stop = true; }
-                    if (stop) a.done[n] = it;
-                }
+                if (lane == 0) resh_decide_cell(a, n, it, rdev);
             }
         }
         grid.sync();
@@ -1419,52 +1476,20 @@ __global__ void __launch_bounds__(RESH_MAX_THREADS) kf_reshape_strips(real *__re
     }
 }
 
-// Reshaping iteration 1 at full occupancy: one strip per block, per-strip
-// partial sums (block order of warps fixed).
+// Reshaping iteration 1 at full occupancy: one strip per block, P = phin
+// (iterate 0) into Q = T, P stored into phi; per-strip partial sums (block
+// order of warps fixed).
 template <typename real, int RB>
 __global__ void __maxnreg__(72) kf_resh_first(const real *__restrict__ P, real *__restrict__ Q,
-                                                                   const real *__restrict__ Jc,
+                                                                   real *__restrict__ phi, const real *__restrict__ Jc,
                                                                    const int *__restrict__ xc,
                                                                    const int *__restrict__ yc, ReshArgs a) {
     extern __shared__ double tile_d[];
     const int n = blockIdx.y, strip = blockIdx.x;
-    const double acc = resh_tile<real, RB>(P, Q, Jc, xc, yc, a, n, strip, (real)a.A, (real)a.B,
+    const double acc = resh_tile<real, RB>(P, P, Q, phi, Jc, xc, yc, a, n, strip, (real)a.A, (real)a.B,
                                            reinterpret_cast<real *>(tile_d));
     const double bs = block_sum_d(acc);
     if (threadIdx.x == 0) a.part[(size_t)n * a.tpc + strip] = bs;
-}
-
-// Loop decision after iteration `it` run by kf_resh_first: one warp per cell,
-// strips summed in order (cell_phase_functions.cpp:554-573).
-__global__ void kf_resh_decide(ReshArgs a, int it) {
-    const int n = blockIdx.x;
-    const double rdev = warp_sum_fixed(a.part + (size_t)n * a.tpc, a.tpc);
-    if (threadIdx.x == 0) {
-        const int k = a.K[n] + 1;
-        a.K[n] = k;
-        bool stop = false;
-        if (k - 1 > a.rimax) { atomicOr(a.err, ERRBIT_RELAX); stop = true; }
-        if (rdev <= a.thr) stop = true;
-        if (!stop && it == a.cap) { atomicOr(a.err, ERRBIT_ITER_CAP); stop = true; }
-        if (stop) a.done[n] = it;
-    }
-}
-
-// Odd iteration counts leave the last iterate in phi; the reference keeps the
-// penultimate one there (the copy at the top of its loop), which is in phin.
-template <typename real, int RB>
-__global__ void __launch_bounds__(RESH_MAX_THREADS) kf_resh_copy(real *__restrict__ phi, const real *__restrict__ phin,
-                                                                  const int *__restrict__ xc,
-                                                                  const int *__restrict__ yc, ReshArgs a) {
-    const int n = blockIdx.y, strip = blockIdx.x, j = threadIdx.x, Z = 2 * a.z;
-    if (!(a.K[n] & 1) || j >= Z) return;
-    const int zi0 = xc[n] - a.z, zj0 = yc[n] - a.z;
-    const size_t base = (size_t)n * a.N * a.N;
-    const int li_end = min(Z, (strip + 1) * RB);
-    for (int li = strip * RB; li < li_end; li++) {
-        const size_t o = base + (size_t)(zi0 + li) * a.N + zj0 + j;
-        phi[o] = phin[o];
-    }
 }
 
 // ---- persistent lumen / ECM update + reshaping
@@ -1544,11 +1569,12 @@ __global__ void kfl_normals(const real *__restrict__ lum, const real *__restrict
     }
 }
 
-// Persistent relaxation of the lumen and ECM fields (cell_phase_functions.cpp:774-869)
+// Relaxation of the lumen and ECM fields (cell_phase_functions.cpp:774-869)
+// from iteration a.it0 on, inside the persistent kernel kf_relax_loops.
 template <typename real>
-__global__ void kf_lum(real *__restrict__ lum, real *__restrict__ lumn, real *__restrict__ ecm,
-                       real *__restrict__ ecmn, const real *__restrict__ Jl, LumArgs a) {
-    cg::grid_group grid = cg::this_grid();
+__device__ __forceinline__ void lum_loops(real *__restrict__ lum, real *__restrict__ lumn, real *__restrict__ ecm,
+                                          real *__restrict__ ecmn, const real *__restrict__ Jl, const LumArgs &a,
+                                          cg::grid_group &grid) {
     const int N = a.N;
     const size_t NN = (size_t)N * N;
     __shared__ int s_last, s_skip;
@@ -1782,21 +1808,53 @@ __global__ void kl_decide(LumArgs a, int it, const double *__restrict__ part, in
 
 // The step ends with lum <- lumn, ECM <- ECMn (run_with_active_gels.cpp:179-181):
 // after an odd iteration count the last iterate already sits in lum / ECM.
+// Copies field f when its count is even and its loop stopped at an iteration
+// in [lo, hi]; 16-byte vectors (cudaMalloc'd fields are 256-byte aligned),
+// then the tail, over threads tid = 0 .. stride-1.
 template <typename real>
-__global__ void kl_copy(real *__restrict__ lum, const real *__restrict__ lumn, real *__restrict__ ecm,
-                        const real *__restrict__ ecmn, const int *__restrict__ K, int N) {
-    const int f = blockIdx.y;
-    if (K[f] & 1) return;
-    real *dst = f ? ecm : lum;
-    const real *src = f ? ecmn : lumn;
-    const size_t NN = (size_t)N * N;
-    // 16-byte vectors (cudaMalloc'd fields are 256-byte aligned), then the tail
+__device__ __forceinline__ void lum_copy_fields(real *__restrict__ lum, const real *__restrict__ lumn,
+                                                real *__restrict__ ecm, const real *__restrict__ ecmn,
+                                                const int *__restrict__ K, const int *__restrict__ done, int N,
+                                                int lo, int hi, size_t tid, size_t stride) {
     typedef typename std::conditional<sizeof(real) == 4, float4, double2>::type vec;
     constexpr int PER = 16 / sizeof(real);
-    const size_t nv = NN / PER;
-    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (size_t)gridDim.x * blockDim.x;
-    for (size_t k = tid; k < nv; k += stride) reinterpret_cast<vec *>(dst)[k] = reinterpret_cast<const vec *>(src)[k];
-    for (size_t k = nv * PER + tid; k < NN; k += stride) dst[k] = src[k];
+    const size_t NN = (size_t)N * N, nv = NN / PER;
+    for (int f = 0; f < 2; f++) {
+        const int d = *(volatile const int *)&done[f];
+        if ((*(volatile const int *)&K[f] & 1) || d < lo || d > hi) continue;
+        real *dst = f ? ecm : lum;
+        const real *src = f ? ecmn : lumn;
+        for (size_t k = tid; k < nv; k += stride) reinterpret_cast<vec *>(dst)[k] = reinterpret_cast<const vec *>(src)[k];
+        for (size_t k = nv * PER + tid; k < NN; k += stride) dst[k] = src[k];
+    }
+}
+// the copy for fields whose loops stopped at iterations 1 .. hi (the regular kernels)
+template <typename real>
+__global__ void kl_copy(real *__restrict__ lum, const real *__restrict__ lumn, real *__restrict__ ecm,
+                        const real *__restrict__ ecmn, const int *__restrict__ K, const int *__restrict__ done, int N,
+                        int hi) {
+    lum_copy_fields<real>(lum, lumn, ecm, ecmn, K, done, N, 1, hi, (size_t)blockIdx.x * blockDim.x + threadIdx.x,
+                          (size_t)gridDim.x * blockDim.x);
+}
+
+// The step's device-side loops in one persistent cooperative kernel: the
+// cells' reshaping from iteration ra.it0 - 1's decision on, then the
+// lumen / ECM relaxation from iteration la.it0 on, then lum <- lumn,
+// ECM <- ECMn for the fields whose loops ran here.
+template <typename real, int RB>
+__global__ void __launch_bounds__(RESH_MAX_THREADS, 2) kf_relax_loops(real *__restrict__ phi, real *__restrict__ phin,
+                                                                    real *__restrict__ T, const real *__restrict__ Jc,
+                                                                    const int *__restrict__ xc,
+                                                                    const int *__restrict__ yc, ReshArgs ra,
+                                                                    real *__restrict__ lum, real *__restrict__ lumn,
+                                                                    real *__restrict__ ecm, real *__restrict__ ecmn,
+                                                                    const real *__restrict__ Jl, LumArgs la) {
+    cg::grid_group grid = cg::this_grid();
+    extern __shared__ double wacc[];          // [warps][Ntot], then the strip tile
+    resh_loops<real, RB>(phi, phin, T, Jc, xc, yc, ra, wacc, grid);
+    lum_loops<real>(lum, lumn, ecm, ecmn, Jl, la, grid);
+    lum_copy_fields<real>(lum, lumn, ecm, ecmn, la.K, la.done, la.N, la.it0, INT_MAX,
+                          (size_t)blockIdx.x * blockDim.x + threadIdx.x, (size_t)gridDim.x * blockDim.x);
 }
 
 // ---- end of step: the periodic ghost ring of rho (boundary_conditions_cells,
@@ -1931,15 +1989,12 @@ struct Fused {
         r->resh_tile = (size_t)3 * (RESH_RB + 2) * (2 * c->zone + 2) * sizeof(real);
         r->resh_smem = (size_t)(r->resh_threads / 32) * c->Ntot * sizeof(double) + r->resh_tile;
         if (r->resh_smem > 200 * 1024) { pfag_set_error("too many cells for the reshaping kernel's per-warp sums"); return PFAG_E_UNSUPPORTED; }
-        PFAG_TRY(smem_at_least((const void *)kf_reshape_strips<real, RESH_RB>, r->resh_smem));
+        PFAG_TRY(smem_at_least((const void *)kf_relax_loops<real, RESH_RB>, r->resh_smem));
         PFAG_TRY(smem_at_least((const void *)kf_resh_first<real, RESH_RB>, r->resh_tile));
-        PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kf_reshape_strips<real, RESH_RB>,
+        PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kf_relax_loops<real, RESH_RB>,
                                                                        r->resh_threads, r->resh_smem));
-        if (per < 1) { pfag_set_error("reshaping kernel cannot be resident with %d threads", r->resh_threads); return PFAG_E_UNSUPPORTED; }
+        if (per < 1) { pfag_set_error("relaxation kernel cannot be resident with %d threads", r->resh_threads); return PFAG_E_UNSUPPORTED; }
         r->coop_r = nsm * std::min(per, 8);
-        PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kf_lum<real>, FT, 0));
-        if (per < 1) { pfag_set_error("lumen/ECM kernel cannot be resident"); return PFAG_E_UNSUPPORTED; }
-        r->coop_l = nsm * std::min(per, 4);
         r->tpc = (2 * c->zone + RESH_RB - 1) / RESH_RB;
         r->ntl = ((c->N + LRB - 1) / LRB) * ((c->N + FT - 1) / FT);
         r->lum_tile = (size_t)3 * (LRB + 2) * (FT + 2) * sizeof(real);
@@ -1957,6 +2012,7 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaMalloc(&r->clsT, (size_t)c->Ntot * mm));
         PFAG_CUDA_CHECK(cudaMalloc(&r->Jc, (size_t)c->Ntot * 2 * W * W * rs));
         PFAG_CUDA_CHECK(cudaMalloc(&r->Jl, 4 * c->ng * rs));
+        if (sizeof(real) == 4) PFAG_CUDA_CHECK(cudaMalloc(&r->G, c->ng * rs));
         PFAG_CUDA_CHECK(cudaMalloc(&r->rect, sizeof(int4) * c->Ntot));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_s, sizeof(double) * c->Ntot * SBLK));
         {
@@ -1965,11 +2021,12 @@ struct Fused {
         }
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_r, sizeof(double) * (size_t)c->Ntot * std::max(r->tpc, r->coop_r)));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_e, sizeof(double) * r->npsi));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->part_l, sizeof(double) * 2 * r->coop_l));
+        PFAG_CUDA_CHECK(cudaMalloc(&r->part_l, sizeof(double) * 2 * r->coop_r));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_lt, sizeof(double) * 2 * r->ntl));
         PFAG_CUDA_CHECK(cudaStreamCreateWithFlags(&r->side, cudaStreamNonBlocking));
         PFAG_CUDA_CHECK(cudaEventCreateWithFlags(&r->ev_psi, cudaEventDisableTiming));
         PFAG_CUDA_CHECK(cudaEventCreateWithFlags(&r->ev_boxA, cudaEventDisableTiming));
+        PFAG_CUDA_CHECK(cudaEventCreateWithFlags(&r->ev_area, cudaEventDisableTiming));
         PFAG_CUDA_CHECK(cudaEventCreateWithFlags(&r->ev_lum, cudaEventDisableTiming));
         PFAG_CUDA_CHECK(cudaMalloc(&r->cK, sizeof(int) * (3 * c->Ntot + 8)));
         r->cdone = r->cK + c->Ntot;
@@ -2012,6 +2069,22 @@ struct Fused {
         return PFAG_OK;
     }
 
+    // the phi update + normals on zone + ring (reads the old rho, like the
+    // spectral solve, which therefore updates rho in place afterwards); runs
+    // after pass A, once the side stream has turned the area partials into f0
+    int launch_update() {
+        cudaStream_t s = c->stream;
+        if (r->fork) PFAG_CUDA_CHECK(cudaStreamWaitEvent(s, r->ev_area, 0));
+        const int z = c->zone, W = 2 * z + 2;
+        dim3 gb((W + UC - 1) / UC, (W + UR - 1) / UR, c->Ntot);
+        pfag_prof_begin(c, "kf_update");
+        kf_update_tiled<real><<<gb, 256, 0, s>>>(R(c->phi), R(c->phin), R(c->rho), R(c->hfunc), c->d_f0,
+                                                 R(c->psi), R(c->hlum), R(c->hecm), c->d_xc, c->d_yc, c->dp,
+                                                 R(r->Jc), R(r->G));
+        PFAG_LAUNCHED(c);
+        return PFAG_OK;
+    }
+
     // enqueue one step (no host synchronisation; capturable)
     int enqueue() {
         cudaStream_t s = c->stream;
@@ -2021,7 +2094,8 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaMemsetAsync(c->d_cacc, 0, sizeof(long long) * 3 * Nt, s));
         pfag_prof_begin(c, "kf_centroid");
         kf_centroid<real><<<dim3(SBLK, Nt), FT, 0, s>>>(R(c->phi), r->rect, N, c->d_cacc); PFAG_LAUNCHED(c);
-        // 2-3. hfunc on the zones, psi, areas, h(lum), h(ECM), sum_ecm partials
+        // 2. centroid finalisation, hfunc on the zones, psi, area partials,
+        //    h(lum), h(ECM), sum_ecm partials
         const int tiles = (N + 31) / 32, tiles_r = (N + PT_R - 1) / PT_R;
         pfag_prof_begin(c, "kf_hpsi");
         kf_hpsi<real><<<dim3(tiles, tiles_r), FT, 0, s>>>(R(c->phi), R(c->hfunc), r->rect, c->d_cacc, c->d_xc,
@@ -2029,15 +2103,13 @@ struct Fused {
                                                          R(c->lum), R(c->ecm), R(c->psi), R(c->hlum), R(c->hecm),
                                                          d.dx * d.dx, r->part_e, r->part_a);
         PFAG_LAUNCHED(c);
-        pfag_prof_begin(c, "kf_area_tiles");
-        kf_area_tiles<<<Nt, 32, 0, s>>>(r->part_a, r->rect, tiles, tiles * tiles_r, d.alpha, d.s0, c->d_s, c->d_f0);
-        PFAG_LAUNCHED(c);
-        // 6a. lumen / ECM update and normals (cell_phase_functions.cpp:372-444,
-        //     :722-771) need only psi and h(lum), h(ECM): they run on the side
-        //     stream beside the phi update and the spectral solve.  Their
-        //     relaxation (6b) rewrites lum and ECM, so it waits for pass A, which
-        //     reads them.  No cooperative kernel runs beside the side stream: the
-        //     main stream joins it before the persistent kernels.
+        // 3. areas and f0, then the lumen / ECM update and normals
+        //    (cell_phase_functions.cpp:372-444, :722-771), which need only psi,
+        //    h(lum) and h(ECM): on the side stream beside pass A, the phi
+        //    update and the rest of the spectral solve.  The relaxation (6)
+        //    rewrites lum and ECM, so it waits for pass A, which reads them.  No
+        //    cooperative kernel runs beside the side stream: the main stream
+        //    joins it before the persistent kernel.
         const bool fork = !pfag_prof_on(c);
         cudaStream_t s2 = fork ? r->side : s;
         r->fork = fork;
@@ -2045,6 +2117,16 @@ struct Fused {
             PFAG_CUDA_CHECK(cudaEventRecord(r->ev_psi, s));
             PFAG_CUDA_CHECK(cudaStreamWaitEvent(s2, r->ev_psi, 0));
         }
+        if (sizeof(real) == 4) {
+            pfag_prof_begin(c, "kf_gel_coupling");
+            kf_gel_coupling<real><<<dim3((N + 31) / 32, (N + 7) / 8), dim3(32, 8), 0, s2>>>(R(c->hlum), R(c->hecm),
+                                                                                        R(r->G), c->dp);
+            PFAG_LAUNCHED(c);
+        }
+        pfag_prof_begin(c, "kf_area_tiles");
+        kf_area_tiles<<<Nt, 32, 0, s2>>>(r->part_a, r->rect, tiles, tiles * tiles_r, d.alpha, d.s0, c->d_s, c->d_f0);
+        PFAG_LAUNCHED(c);
+        if (fork) PFAG_CUDA_CHECK(cudaEventRecord(r->ev_area, s2));
         PFAG_CUDA_CHECK(cudaMemsetAsync(r->lK, 0, sizeof(int) * 8, s2));
         LumArgs la{};
         la.N = N; la.rimax = c->p.rimax; la.cap = c->relax_cap; la.npsi = r->npsi;
@@ -2068,18 +2150,8 @@ struct Fused {
             kfl_normals<real><<<gb, tb, 0, s2>>>(R(c->lum), R(c->lumn), R(c->ecm), R(c->ecmn), R(r->Jl), N, d.dx);
             PFAG_LAUNCHED(c);
         }
-        // 4. phi update + normals on zone + ring (reads the old rho, like the
-        //    spectral solve, which therefore updates rho in place afterwards)
-        {
-            const int W = 2 * z + 2;
-            dim3 gb((W + UC - 1) / UC, (W + UR - 1) / UR, Nt);
-            pfag_prof_begin(c, "kf_update");
-            kf_update_tiled<real><<<gb, 256, 0, s>>>(R(c->phi), R(c->phin), R(c->rho), R(c->hfunc), c->d_f0,
-                                                     R(c->psi), R(c->hlum), R(c->hecm), c->d_xc, c->d_yc, c->dp,
-                                                     R(r->Jc));
-            PFAG_LAUNCHED(c);
-        }
-        // 5. spectral solve; pass E writes the new rho over each box in place
+        // 4-5. spectral solve with the phi update after its pass A; the last
+        //    column pass writes the new rho over each box in place
         //    (rho <- rhon of run_with_active_gels.cpp:175-178 on the box)
         const BoxArgs ba = box_args(c);
         const int Rr = r->rows_blk, G = r->grp_cols;
@@ -2094,6 +2166,7 @@ struct Fused {
                                                              c->d_yc, ba, Rr, Y1, Y2, R(r->Rb), r->clsT);
         PFAG_LAUNCHED(c);
         if (r->fork) PFAG_CUDA_CHECK(cudaEventRecord(r->ev_boxA, s));
+        PFAG_TRY(launch_update());
         const int ngrp = (M / 2 + 1 + G - 1) / G;
         pfag_prof_begin(c, "kf_boxB");
         kf_boxB<real><<<dim3(ngrp, Nt), FT, r->smemB, s>>>(Y1, Y2, r->clsT, ba, G); PFAG_LAUNCHED(c);
@@ -2109,10 +2182,11 @@ struct Fused {
                                                              ba, Rr);
         PFAG_LAUNCHED(c);
         }
-        // 6b. lumen / ECM relaxation: iterations 1 .. LUM_REGULAR as
-        //     full-occupancy kernels on the side stream once pass A has read lum
-        //     and ECM; the rest (if a field still moves) in the persistent kernel
-        //     after the join below
+        // 6. lumen / ECM relaxation: iterations 1 .. LUM_REGULAR as
+        //    full-occupancy kernels on the side stream once pass A has read lum
+        //    and ECM, and lum <- lumn, ECM <- ECMn for the fields that stopped
+        //    there; the rest (if a field still moves) in the persistent kernel
+        //    after the join below
         if (fork) PFAG_CUDA_CHECK(cudaStreamWaitEvent(s2, r->ev_boxA, 0));
         for (int it = 1; it <= LUM_REGULAR; it++) {
             pfag_prof_begin(c, "kl_relax");
@@ -2123,8 +2197,14 @@ struct Fused {
             kl_decide<<<2, 32, 0, s2>>>(la, it, r->part_lt, r->ntl);
             PFAG_LAUNCHED(c);
         }
+        pfag_prof_begin(c, "kl_copy");
+        kl_copy<real><<<296, FT, 0, s2>>>(R(c->lum), R(c->lumn), R(c->ecm), R(c->ecmn), r->lK, r->ldone, N,
+                                          LUM_REGULAR);
+        PFAG_LAUNCHED(c);
         if (fork) PFAG_CUDA_CHECK(cudaEventRecord(r->ev_lum, s2));
-        // 7. reshaping of the cells
+        // 7. reshaping of the cells: iteration 1 at full occupancy, then the
+        //    persistent kernel (its decision, iterations 2.., and the lumen /
+        //    ECM iterations beyond LUM_REGULAR)
         PFAG_CUDA_CHECK(cudaMemsetAsync(r->cK, 0, sizeof(int) * 3 * Nt, s));
         {
             ReshArgs ra{};
@@ -2132,39 +2212,25 @@ struct Fused {
             ra.rimax = c->p.rimax; ra.cap = c->relax_cap;
             ra.A = d.A_resh; ra.B = d.B_resh; ra.scale = d.dx * d.dx / (double)d.Ncur; ra.thr = d.thr_cells;
             ra.K = r->cK; ra.done = r->cdone; ra.cnt = r->ccnt; ra.part = r->part_r; ra.err = c->d_err;
-            real *a0 = R(c->phi), *a1 = R(c->phin);
-            const real *a2 = R(r->Jc);
-            const int *a3 = c->d_xc, *a4 = c->d_yc;
             ra.it0 = 2;
+            la.it0 = LUM_REGULAR + 1;
+            real *T = R(c->rhon);          // the fused path keeps rho in place: rhon is the reshaping scratch
             const dim3 gs(r->tpc, Nt);
             pfag_prof_begin(c, "kf_resh_first");
-            kf_resh_first<real, RESH_RB><<<gs, r->resh_threads, r->resh_tile, s>>>(R(c->phin), R(c->phi), R(r->Jc), c->d_xc,
-                                                                        c->d_yc, ra);
+            kf_resh_first<real, RESH_RB><<<gs, r->resh_threads, r->resh_tile, s>>>(R(c->phin), T, R(c->phi), R(r->Jc),
+                                                                                    c->d_xc, c->d_yc, ra);
             PFAG_LAUNCHED(c);
-            pfag_prof_begin(c, "kf_resh_decide");
-            kf_resh_decide<<<Nt, 32, 0, s>>>(ra, 1);
-            PFAG_LAUNCHED(c);
-            void *args[] = {&a0, &a1, (void *)&a2, (void *)&a3, (void *)&a4, &ra};
+            real *a0 = R(c->phi), *a1 = R(c->phin), *a2 = T;
+            const real *a3 = R(r->Jc);
+            const int *a4 = c->d_xc, *a5 = c->d_yc;
+            real *b0 = R(c->lum), *b1 = R(c->lumn), *b2 = R(c->ecm), *b3 = R(c->ecmn);
+            const real *b4 = R(r->Jl);
+            void *args[] = {&a0, &a1, &a2, (void *)&a3, (void *)&a4, (void *)&a5, &ra,
+                            &b0, &b1, &b2, &b3, (void *)&b4, &la};
             if (fork) PFAG_CUDA_CHECK(cudaStreamWaitEvent(s, r->ev_lum, 0));   // join the side stream
-            pfag_prof_begin(c, "kf_reshape");
-            PFAG_TRY(launch_coop_t((const void *)kf_reshape_strips<real, RESH_RB>, &r->coop_r, r->resh_threads, args,
+            pfag_prof_begin(c, "kf_relax_loops");
+            PFAG_TRY(launch_coop_t((const void *)kf_relax_loops<real, RESH_RB>, &r->coop_r, r->resh_threads, args,
                                    r->resh_smem, s));
-            PFAG_LAUNCHED(c);
-            pfag_prof_begin(c, "kf_resh_copy");
-            kf_resh_copy<real, RESH_RB><<<gs, r->resh_threads, 0, s>>>(R(c->phi), R(c->phin), c->d_xc, c->d_yc, ra);
-            PFAG_LAUNCHED(c);
-        }
-        // 7b. lumen / ECM iterations beyond LUM_REGULAR, and lum <- lumn, ECM <- ECMn
-        {
-            la.it0 = LUM_REGULAR + 1;
-            real *a0 = R(c->lum), *a1 = R(c->lumn), *a2 = R(c->ecm), *a3 = R(c->ecmn);
-            const real *a4 = R(r->Jl);
-            void *args[] = {&a0, &a1, &a2, &a3, (void *)&a4, &la};
-            pfag_prof_begin(c, "kf_lum");
-            PFAG_TRY(launch_coop_t((const void *)kf_lum<real>, &r->coop_l, FT, args, 0, s));
-            PFAG_LAUNCHED(c);
-            pfag_prof_begin(c, "kl_copy");
-            kl_copy<real><<<dim3(296, 2), FT, 0, s>>>(R(c->lum), R(c->lumn), R(c->ecm), R(c->ecmn), r->lK, N);
             PFAG_LAUNCHED(c);
         }
         // 8. periodic ghost ring of rho (boundary_conditions_cells(rhon),
@@ -2214,6 +2280,7 @@ struct Fused {
                                                           ba, Y1, Y2, R(r->Rb), r->clsT);
         PFAG_LAUNCHED(c);
         if (r->fork) PFAG_CUDA_CHECK(cudaEventRecord(r->ev_boxA, s));
+        PFAG_TRY(launch_update());
         pfag_prof_begin(c, "kf_boxB");
         kr_boxB<real, MM, GB><<<dim3((MM / 2 + 1 + GB - 1) / GB, Nt), 256, smB, s>>>(Y1, Y2, r->clsT, ba);
         PFAG_LAUNCHED(c);
@@ -2232,11 +2299,10 @@ struct Fused {
     int stats() {
         const int Nt = c->Ntot;
         if (std::getenv("PFAG_DEBUG_COOP")) {
-            cudaFuncAttributes fr{}, fl{};
-            cudaFuncGetAttributes(&fr, (const void *)kf_reshape_strips<real, RESH_RB>);
-            cudaFuncGetAttributes(&fl, (const void *)kf_lum<real>);
-            std::fprintf(stderr, "pfag coop: reshape %d blocks x %d threads (%d regs), lum %d blocks x %d (%d regs)\n",
-                         r->coop_r, r->resh_threads, fr.numRegs, r->coop_l, FT, fl.numRegs);
+            cudaFuncAttributes fr{};
+            cudaFuncGetAttributes(&fr, (const void *)kf_relax_loops<real, RESH_RB>);
+            std::fprintf(stderr, "pfag coop: relaxation loops %d blocks x %d threads (%d regs)\n", r->coop_r,
+                         r->resh_threads, fr.numRegs);
         }
         std::vector<int> h(3 * Nt + 8);
         PFAG_CUDA_CHECK(cudaMemcpyAsync(h.data(), r->cK, sizeof(int) * (3 * Nt + 8), cudaMemcpyDeviceToHost, c->stream));
