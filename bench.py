@@ -188,13 +188,13 @@ def kernel_bytes(cfg, precision: int, iters: dict) -> dict:
         "kf_gel_coupling": N * N * 3 * w,
         # reshaping iteration 1: read P and J (x, y), write Q and phi (P), over every zone
         "kf_resh_first": zone * 5 * w,
-        # per launch: further reshaping iterations (read P, J_x, J_y, write Q, phi) and
-        # lumen / ECM iterations beyond the second (read P, J_x, J_y, write Q)
-        "kf_relax_loops": ((2 * z) * (2 * z) * 5 * w * (cell_it - n) +
+        # per launch: further reshaping iterations (read P, J_x, J_y, write Q, phi), the next
+        # step's centroid sums (read phi over B_n, about a zone) and lumen / ECM iterations
+        # beyond the second (read P, J_x, J_y, write Q)
+        "kf_relax_loops": ((2 * z) * (2 * z) * 5 * w * (cell_it - n) + zone * w +
                            N * N * 4 * w * (max(lum_it - 2, 0) + max(ecm_it - 2, 0))),
         # reads phi on the zones (hfunc elsewhere in B_n), lum, ECM; writes hfunc (zones), psi, h(lum), h(ECM)
         "kf_hpsi": N * N * (2 * w + 3 * w) + zone * 2 * w,
-        "kf_centroid": zone * w,
         # read lum, ECM, psi, h(lum), h(ECM); write lumn, ECMn
         "kfl_update": N * N * 7 * w,
         # read lum, lumn, ECM, ECMn; write 4 normal components

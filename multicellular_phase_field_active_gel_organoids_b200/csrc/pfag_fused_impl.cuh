@@ -765,7 +765,7 @@ template <int M> struct BoxGeom {
 
 // Pass A on register FFTs: one thread group per box row.
 template <typename real, int M>
-__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxA(const real *__restrict__ phi, const real *__restrict__ rho,
+__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) kr_boxA(const real *__restrict__ phi, const real *__restrict__ rho,
                                                const real *__restrict__ lum, const real *__restrict__ ecm,
                                                const int *__restrict__ xc, const int *__restrict__ yc, BoxArgs a,
                                                typename Cplx<real>::type *__restrict__ Y1,
@@ -903,10 +903,10 @@ __device__ __forceinline__ void columns_fft(cx *Z, int nseq_pad, const cx *tw) {
 // Thread t always handles slot t % NSP and rows t / NSP + k * (blockDim / NSP),
 // so the loop has shift-only indexing and independent loads; slots past the
 // block's columns are zero and never stored.
-template <typename cx, int M, int NSP>
+template <typename cx, int M, int NSP, int BT = 256>
 __device__ __forceinline__ void load_cols_fixed(cx *dst, const cx *__restrict__ src, const ColSlots &cs) {
-    constexpr int S = M + 1, STEP = 256 / NSP;
-    static_assert(NSP <= 256 && (NSP & (NSP - 1)) == 0, "NSP must be a power of two <= 256");
+    constexpr int S = M + 1, STEP = BT / NSP;
+    static_assert(NSP <= BT && (NSP & (NSP - 1)) == 0, "NSP must be a power of two <= the block size");
     const int sl = threadIdx.x % NSP, i0 = threadIdx.x / NSP;
     const bool live = sl < cs.ns;
     const int col = live ? cs.col[sl] : 0;
@@ -919,9 +919,9 @@ __device__ __forceinline__ void load_cols_fixed(cx *dst, const cx *__restrict__ 
     }
 }
 
-template <typename cx, int M, int NSP>
+template <typename cx, int M, int NSP, int BT = 256>
 __device__ __forceinline__ void store_cols_fixed(cx *__restrict__ dstg, const cx *src, const ColSlots &cs) {
-    constexpr int S = M + 1, STEP = 256 / NSP;
+    constexpr int S = M + 1, STEP = BT / NSP;
     const int sl = threadIdx.x % NSP, i0 = threadIdx.x / NSP;
     if (sl >= cs.ns) return;
     const int col = cs.col[sl];
@@ -1024,7 +1024,7 @@ template <int M> struct BoxGeomD2 {
     static constexpr int NSQ = COLS / 2;                               // complex sequences per block
 };
 template <typename real, int M>
-__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxD2(const real *__restrict__ X, real *__restrict__ rho,
+__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) kr_boxD2(const real *__restrict__ X, real *__restrict__ rho,
                                                 const real *__restrict__ Rb, const int *__restrict__ xc,
                                                 const int *__restrict__ yc, BoxArgs a) {
     typedef typename Cplx<real>::type cx;
@@ -1116,8 +1116,8 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxD2(const
     }
 }
 
-template <typename real, int M, int G>
-__global__ void __launch_bounds__(256) kr_boxB(typename Cplx<real>::type *__restrict__ Y1,
+template <typename real, int M, int G, int BT>
+__global__ void __launch_bounds__(BT, 1024 / BT) kr_boxB(typename Cplx<real>::type *__restrict__ Y1,
                                                const typename Cplx<real>::type *__restrict__ Y2,
                                                const unsigned char *__restrict__ clsT, BoxArgs a) {
     typedef typename Cplx<real>::type cx;
@@ -1136,8 +1136,8 @@ __global__ void __launch_bounds__(256) kr_boxB(typename Cplx<real>::type *__rest
     constexpr int NZ2 = ((G + WG - 1) / WG) * WG;   // padded to whole warps
     static_assert((NSP + NZ2) % WG == 0, "slot count must be a multiple of the thread groups per warp");
     cx *Z1 = tw + M, *Z2 = Z1 + (size_t)NSP * S;
-    load_cols_fixed<cx, M, NSP>(Z1, Y1 + (size_t)n * M * M, cs);
-    load_cols_fixed<cx, M, NZ2>(Z2, Y2 + (size_t)n * M * M, cs);
+    load_cols_fixed<cx, M, NSP, BT>(Z1, Y1 + (size_t)n * M * M, cs);
+    load_cols_fixed<cx, M, NZ2, BT>(Z2, Y2 + (size_t)n * M * M, cs);
     __syncthreads();
     columns_fft<cx, M, false>(Z1, NSP + NZ2, tw);   // Z2 follows Z1 with the same stride
     __syncthreads();
@@ -1174,7 +1174,7 @@ __global__ void __launch_bounds__(256) kr_boxB(typename Cplx<real>::type *__rest
     __syncthreads();
     columns_fft<cx, M, true>(Z1, NSP, tw);
     __syncthreads();
-    store_cols_fixed<cx, M, NSP>(Y1 + (size_t)n * M * M, Z1, cs);
+    store_cols_fixed<cx, M, NSP, BT>(Y1 + (size_t)n * M * M, Z1, cs);
 }
 
 // ---- phi update (cell_phase_functions.cpp:126-217) + normals
@@ -1486,6 +1486,7 @@ __global__ void __maxnreg__(72) kf_resh_first(const real *__restrict__ P, real *
                                                                    const int *__restrict__ yc, ReshArgs a) {
     extern __shared__ double tile_d[];
     const int n = blockIdx.y, strip = blockIdx.x;
+    if (strip == 0 && threadIdx.x == 0) { a.K[n] = 0; a.done[n] = 0; }   // read from the next kernel on
     const double acc = resh_tile<real, RB>(P, P, Q, phi, Jc, xc, yc, a, n, strip, (real)a.A, (real)a.B,
                                            reinterpret_cast<real *>(tile_d));
     const double bs = block_sum_d(acc);
@@ -1528,6 +1529,9 @@ __global__ void kfl_update(const real *__restrict__ lum, const real *__restrict_
                            const real *__restrict__ he, const double *__restrict__ sum_ecm, LumArgs a) {
     const int N = a.N;
     const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0 && j == 0) {            // this step's loop counters of both fields (read from kl_relax on)
+        for (int f = 0; f < 2; f++) { a.K[f] = 0; a.done[f] = 0; a.cnt[f] = 0; }
+    }
     if (i >= N || j >= N) return;
     const size_t k = (size_t)i * N + j;
     if (i == 0 || i == N - 1 || j == 0 || j == N - 1) { lumn[k] = (real)0.0; ecmn[k] = (real)1.0; return; }
@@ -1837,10 +1841,44 @@ __global__ void kl_copy(real *__restrict__ lum, const real *__restrict__ lumn, r
                           (size_t)gridDim.x * blockDim.x);
 }
 
+// The next step's centroid sums (find_centres_cells, useful_functions.cpp:
+// 193-227) over each cell's support rectangle of the reshaped phi: one warp
+// per rectangle row, exact integer sums added atomically into acc (zeroed
+// before the grid barrier that precedes this).  Nothing writes phi between
+// the end of the reshaping loops and the next step's centroids.
+template <typename real>
+__device__ __forceinline__ void centroid_rows(const real *__restrict__ phi, const int4 *__restrict__ rect, int N,
+                                              int Ntot, long long *__restrict__ acc) {
+    const int lane = threadIdx.x & 31;
+    const int nw = blockDim.x >> 5;
+    const int nwt = gridDim.x * nw;
+    for (int t = blockIdx.x * nw + (threadIdx.x >> 5); t < Ntot * N; t += nwt) {
+        const int n = t / N, i = t - n * N;
+        const int4 r = rect[n];
+        if (i < r.x || i >= r.y) continue;                       // warp-uniform
+        const real *p = phi + (size_t)n * N * N + (size_t)i * N;
+        int cnt = 0, sy = 0;                                     // at most N sites of index < N per row
+#pragma unroll 4
+        for (int j = r.z + lane; j < r.w; j += 32) {
+            if (p[j] > (real)0.5) { cnt++; sy += j; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+            sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        }
+        if (lane == 0 && cnt) {
+            atomicAdd((unsigned long long *)&acc[3 * n + 0], (unsigned long long)cnt);
+            atomicAdd((unsigned long long *)&acc[3 * n + 1], (unsigned long long)((long long)cnt * i));
+            atomicAdd((unsigned long long *)&acc[3 * n + 2], (unsigned long long)sy);
+        }
+    }
+}
+
 // The step's device-side loops in one persistent cooperative kernel: the
-// cells' reshaping from iteration ra.it0 - 1's decision on, then the
-// lumen / ECM relaxation from iteration la.it0 on, then lum <- lumn,
-// ECM <- ECMn for the fields whose loops ran here.
+// cells' reshaping from iteration ra.it0 - 1's decision on, the next step's
+// centroid sums of the reshaped cells, the lumen / ECM relaxation from
+// iteration la.it0 on, then lum <- lumn, ECM <- ECMn for the fields whose
+// loops ran here.
 template <typename real, int RB>
 __global__ void __launch_bounds__(RESH_MAX_THREADS, 2) kf_relax_loops(real *__restrict__ phi, real *__restrict__ phin,
                                                                     real *__restrict__ T, const real *__restrict__ Jc,
@@ -1848,10 +1886,15 @@ __global__ void __launch_bounds__(RESH_MAX_THREADS, 2) kf_relax_loops(real *__re
                                                                     const int *__restrict__ yc, ReshArgs ra,
                                                                     real *__restrict__ lum, real *__restrict__ lumn,
                                                                     real *__restrict__ ecm, real *__restrict__ ecmn,
-                                                                    const real *__restrict__ Jl, LumArgs la) {
+                                                                    const real *__restrict__ Jl, LumArgs la,
+                                                                    const int4 *__restrict__ rect,
+                                                                    long long *__restrict__ cacc) {
     cg::grid_group grid = cg::this_grid();
     extern __shared__ double wacc[];          // [warps][Ntot], then the strip tile
-    resh_loops<real, RB>(phi, phin, T, Jc, xc, yc, ra, wacc, grid);
+    if (blockIdx.x == 0)                      // consumed by this step's kf_hpsi; refilled below
+        for (int k = threadIdx.x; k < 3 * ra.Ntot; k += blockDim.x) cacc[k] = 0;
+    resh_loops<real, RB>(phi, phin, T, Jc, xc, yc, ra, wacc, grid);   // ends with a grid barrier
+    centroid_rows<real>(phi, rect, ra.N, ra.Ntot, cacc);
     lum_loops<real>(lum, lumn, ecm, ecmn, Jl, la, grid);
     lum_copy_fields<real>(lum, lumn, ecm, ecmn, la.K, la.done, la.N, la.it0, INT_MAX,
                           (size_t)blockIdx.x * blockDim.x + threadIdx.x, (size_t)gridDim.x * blockDim.x);
@@ -2090,12 +2133,9 @@ struct Fused {
         cudaStream_t s = c->stream;
         const int N = c->N, Nt = c->Ntot, M = c->M, z = c->zone;
         const DevParams &d = c->dp;
-        // 1. centroids over B_n
-        PFAG_CUDA_CHECK(cudaMemsetAsync(c->d_cacc, 0, sizeof(long long) * 3 * Nt, s));
-        pfag_prof_begin(c, "kf_centroid");
-        kf_centroid<real><<<dim3(SBLK, Nt), FT, 0, s>>>(R(c->phi), r->rect, N, c->d_cacc); PFAG_LAUNCHED(c);
-        // 2. centroid finalisation, hfunc on the zones, psi, area partials,
-        //    h(lum), h(ECM), sum_ecm partials
+        // 1-2. centroids (from the sums the previous step's persistent kernel,
+        //    or the upload, left over B_n), hfunc on the zones, psi, area
+        //    partials, h(lum), h(ECM), sum_ecm partials
         const int tiles = (N + 31) / 32, tiles_r = (N + PT_R - 1) / PT_R;
         pfag_prof_begin(c, "kf_hpsi");
         kf_hpsi<real><<<dim3(tiles, tiles_r), FT, 0, s>>>(R(c->phi), R(c->hfunc), r->rect, c->d_cacc, c->d_xc,
@@ -2127,7 +2167,6 @@ struct Fused {
         kf_area_tiles<<<Nt, 32, 0, s2>>>(r->part_a, r->rect, tiles, tiles * tiles_r, d.alpha, d.s0, c->d_s, c->d_f0);
         PFAG_LAUNCHED(c);
         if (fork) PFAG_CUDA_CHECK(cudaEventRecord(r->ev_area, s2));
-        PFAG_CUDA_CHECK(cudaMemsetAsync(r->lK, 0, sizeof(int) * 8, s2));
         LumArgs la{};
         la.N = N; la.rimax = c->p.rimax; la.cap = c->relax_cap; la.npsi = r->npsi;
         la.dx = d.dx; la.dt = d.dt; la.tau_lum = d.tau_lum; la.xi_lum = d.xi_lum;
@@ -2205,7 +2244,6 @@ struct Fused {
         // 7. reshaping of the cells: iteration 1 at full occupancy, then the
         //    persistent kernel (its decision, iterations 2.., and the lumen /
         //    ECM iterations beyond LUM_REGULAR)
-        PFAG_CUDA_CHECK(cudaMemsetAsync(r->cK, 0, sizeof(int) * 3 * Nt, s));
         {
             ReshArgs ra{};
             ra.N = N; ra.z = z; ra.Ntot = Nt; ra.tpc = r->tpc;
@@ -2225,8 +2263,10 @@ struct Fused {
             const int *a4 = c->d_xc, *a5 = c->d_yc;
             real *b0 = R(c->lum), *b1 = R(c->lumn), *b2 = R(c->ecm), *b3 = R(c->ecmn);
             const real *b4 = R(r->Jl);
+            const int4 *c0 = r->rect;
+            long long *c1 = c->d_cacc;
             void *args[] = {&a0, &a1, &a2, (void *)&a3, (void *)&a4, (void *)&a5, &ra,
-                            &b0, &b1, &b2, &b3, (void *)&b4, &la};
+                            &b0, &b1, &b2, &b3, (void *)&b4, &la, (void *)&c0, &c1};
             if (fork) PFAG_CUDA_CHECK(cudaStreamWaitEvent(s, r->ev_lum, 0));   // join the side stream
             pfag_prof_begin(c, "kf_relax_loops");
             PFAG_TRY(launch_coop_t((const void *)kf_relax_loops<real, RESH_RB>, &r->coop_r, r->resh_threads, args,
@@ -2267,7 +2307,7 @@ struct Fused {
         const int nz2 = ((GB + BG::WG - 1) / BG::WG) * BG::WG;
         const size_t smB = (MM + (size_t)(nsB + nz2) * (MM + 1)) * cs;
         PFAG_TRY(smem_at_least((const void *)kr_boxA<real, MM>, smA));
-        PFAG_TRY(smem_at_least((const void *)kr_boxB<real, MM, GB>, smB));
+        PFAG_TRY(smem_at_least((const void *)kr_boxB<real, MM, GB, 256>, smB));
         typedef BoxGeomD2<MM> BD;
         constexpr int NSP2 = (BD::NSQ % BG::WG == 0) ? BD::NSQ : ((BD::NSQ + BG::WG - 1) / BG::WG) * BG::WG;
         const size_t smD2 = (MM + (size_t)NSP2 * (MM + 1)) * cs;
@@ -2282,7 +2322,7 @@ struct Fused {
         if (r->fork) PFAG_CUDA_CHECK(cudaEventRecord(r->ev_boxA, s));
         PFAG_TRY(launch_update());
         pfag_prof_begin(c, "kf_boxB");
-        kr_boxB<real, MM, GB><<<dim3((MM / 2 + 1 + GB - 1) / GB, Nt), 256, smB, s>>>(Y1, Y2, r->clsT, ba);
+        kr_boxB<real, MM, GB, 256><<<dim3((MM / 2 + 1 + GB - 1) / GB, Nt), 256, smB, s>>>(Y1, Y2, r->clsT, ba);
         PFAG_LAUNCHED(c);
         real *X = (real *)r->Y2;          // pass B is done with Y2: Fx, then the row term
         pfag_prof_begin(c, "kf_boxC");
