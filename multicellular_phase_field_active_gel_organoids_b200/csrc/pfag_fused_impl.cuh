@@ -88,6 +88,8 @@ struct FusedRes {
     bool fork;
     int npsi;
     int coop_r;             // co-resident block count of the persistent kernel
+    long upd_warps;         // co-resident warps of kf_update_rows (FP32)
+    size_t upd_smem;        // its row ring
     int logm, rows_blk, grp_cols;
     size_t smemA, smemB, smemC, smemD, smemE;
     bool ring_pending;      // the rho ghost ring still has to be made to match its sources
@@ -1310,6 +1312,135 @@ __global__ void __launch_bounds__(256) kf_update_tiled(const real *__restrict__ 
     }
 }
 
+// FP32 phi update + normals (cell_phase_functions.cpp:126-217,
+// useful_functions.cpp:356-388) as a sliding window down the rows: a warp
+// task is 30 columns x `rb` rows of one cell's zone + ring; lane l holds
+// column cg*30 + l - 1 (lanes 0 and 31 only supply the left/right
+// neighbours, read with warp shuffles).  Each thread keeps phi, rho and
+// T = psi - hfunc of rows r-1, r, r+1 in registers; rows r+2 .. r+1+UPD_DEPTH
+// of phi, rho, psi, hfunc and G are in flight as per-thread cp.async copies
+// into a ring of UPD_DEPTH+1 shared-memory slots (a thread reads back only
+// its own elements: no block barrier), one commit group per row; a row's
+// slot is refilled one iteration after it was read.  Sites with a periodic
+// ghost neighbour (a region touching the grid's ghost ring) take their
+// normals from global memory through the ghost map.
+constexpr int UPD_COLS = 30, UPD_DEPTH = 6, UPD_SLOTS = UPD_DEPTH + 1, UPD_THREADS = 256;
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int K>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
+
+template <typename real>
+__global__ void __launch_bounds__(UPD_THREADS, 5) kf_update_rows(const real *__restrict__ phi, real *__restrict__ phin,
+                                                                 const real *__restrict__ rho,
+                                                                 const real *__restrict__ hfunc,
+                                                                 const double *__restrict__ f0,
+                                                                 const real *__restrict__ psi,
+                                                                 const real *__restrict__ G, const int *__restrict__ xc,
+                                                                 const int *__restrict__ yc, DevParams P,
+                                                                 real *__restrict__ Jc, int cgroups, int rchunks,
+                                                                 int rb) {
+    static_assert(sizeof(real) == 4, "the FP64 build keeps kf_update_tiled (reference operation order)");
+    extern __shared__ float upd_ring[];                           // [UPD_SLOTS][5][UPD_THREADS]
+    const int lane = threadIdx.x & 31;
+    const int task = blockIdx.x * (UPD_THREADS >> 5) + (threadIdx.x >> 5);
+    const int N = P.N, z = P.zone, W = 2 * z + 2;
+    if (task >= P.Ntot * cgroups * rchunks) return;              // whole warps
+    const int n = task / (cgroups * rchunks);
+    const int rem = task - n * cgroups * rchunks;
+    const int cg = rem / rchunks, rc = rem - cg * rchunks;
+    const int cc = cg * UPD_COLS + lane - 1;                      // region column of this lane
+    const int r0 = rc * rb, r1 = min(W, r0 + rb);
+    const int gi0 = xc[n] - z - 1, gj0 = yc[n] - z - 1;         // region origin (grid)
+    const int gj = gj0 + cc;
+    const int gjc = min(max(gj, 0), N - 1);                      // clamped load column
+    const bool out = lane >= 1 && lane <= UPD_COLS && cc < W;
+    const size_t base = (size_t)n * N * N;
+    // per-cell planes and 32-bit offsets (N^2 < 2^31)
+    const real *__restrict__ pp = phi + base, *__restrict__ pr = rho + base, *__restrict__ ph = hfunc + base;
+    auto row = [&](int r) { return (unsigned)(min(max(gi0 + r, 0), N - 1) * N + gjc); };
+    float *ring = upd_ring + threadIdx.x;
+    auto issue = [&](int r, int slot) {                          // row r into a ring slot, one commit group
+        if (r <= r1) {
+            const unsigned a = row(r);
+            float *d = ring + slot * 5 * UPD_THREADS;
+            cp_async_elem(d, pp + a);
+            cp_async_elem(d + UPD_THREADS, pr + a);
+            cp_async_elem(d + 2 * UPD_THREADS, psi + a);
+            cp_async_elem(d + 3 * UPD_THREADS, ph + a);
+            cp_async_elem(d + 4 * UPD_THREADS, G + a);
+        }
+        cp_async_commit();
+    };
+    const real dt_tau = (real)P.dt_tau, beta = (real)P.beta, eta = (real)P.eta, iq4 = (real)P.inv_q4;
+    const real c4 = (real)(1.0 / P.dx / P.dx / 4.0), inv2dx = (real)(1.0 / (2.0 * P.dx));
+    const real kcpl = (real)P.k_cpl, i2s2 = (real)P.inv_2s2;
+    const real fn0 = (real)f0[n];
+    real *Jx = Jc + (size_t)n * 2 * W * W, *Jy = Jx + (size_t)W * W;
+    // rows r0+2 .. r0+1+UPD_DEPTH in flight (slot of row x: (x - r0 - 2) mod UPD_SLOTS)
+#pragma unroll
+    for (int k = 0; k < UPD_DEPTH; k++) issue(r0 + 2 + k, k);
+    // window rows r-1, r, r+1 (phi p, rho q, T t) and G of row r
+    real p0, p1, p2, q0, q1, q2, t0, t1, t2, g1;
+    {
+        const unsigned a = row(r0 - 1), b = row(r0), c = row(r0 + 1);
+        p0 = pp[a]; p1 = pp[b]; p2 = pp[c];
+        q0 = pr[a]; q1 = pr[b]; q2 = pr[c];
+        t0 = psi[a] - ph[a]; t1 = psi[b] - ph[b]; t2 = psi[c] - ph[c];
+        g1 = G[b];
+    }
+    real g2 = G[row(r0 + 1)];
+    real tl0 = __shfl_up_sync(0xffffffffu, t0, 1), tr0 = __shfl_down_sync(0xffffffffu, t0, 1);
+    real tl1 = __shfl_up_sync(0xffffffffu, t1, 1), tr1 = __shfl_down_sync(0xffffffffu, t1, 1);
+    int rd = 0;                                                   // slot of row r+2
+    for (int r = r0; r < r1; r++) {
+        const int gi = gi0 + r;
+        const bool zone = r >= 1 && r <= 2 * z && cc >= 1 && cc <= 2 * z;
+        const real tl2 = __shfl_up_sync(0xffffffffu, t2, 1), tr2 = __shfl_down_sync(0xffffffffu, t2, 1);
+        const real pl = __shfl_up_sync(0xffffffffu, p1, 1), prt = __shfl_down_sync(0xffffffffu, p1, 1);
+        const real ql = __shfl_up_sync(0xffffffffu, q1, 1), qr = __shfl_down_sync(0xffffffffu, q1, 1);
+        if (out) {
+            real ja, jb;
+            if (gi >= 1 && gi <= N - 2 && gj >= 1 && gj <= N - 2) {
+                ja = p2 - p0;
+                jb = prt - pl;
+            } else {
+                const unsigned c = (unsigned)(ghost_src(gi, N) * N + ghost_src(gj, N));
+                ja = pp[c + N] - pp[c - N];
+                jb = pp[c + 1] - pp[c - 1];
+            }
+            const real qq = c4 * (ja * ja + jb * jb);
+            const real rg = (qq > (real)0.0) ? rsqrtf(qq) : (real)0.0;
+            const unsigned jo = (unsigned)(r * W + cc);
+            Jx[jo] = inv2dx * ja * rg;
+            Jy[jo] = inv2dx * jb * rg;
+            const real f = p1;
+            real pn = f;
+            if (zone) {
+                if (qq > (real)0.0) {
+                    const real d = f - (real)0.5;
+                    pn -= kcpl * __expf(-d * d * i2s2) * ((q2 - q0) * ja + (qr - ql) * jb) * rg;
+                }
+                const real LT = lap9<real>(t1, t2, t0, tr1, tl1, tr2, tl2, tl0, tr0);
+                pn += dt_tau * f * ((real)1.0 - f) * (fn0 - beta * t1 + eta * LT * iq4 + g1);
+            }
+            phin[base + (unsigned)(gi * N + gj)] = pn;
+        }
+        // slide the window down one row: row r+2 from its slot, then refill the
+        // slot read one iteration ago with row r+2+UPD_DEPTH
+        cp_async_wait<UPD_DEPTH - 1>();
+        const float *sv = ring + rd * 5 * UPD_THREADS;
+        p0 = p1; p1 = p2; p2 = sv[0];
+        q0 = q1; q1 = q2; q2 = sv[UPD_THREADS];
+        t0 = t1; t1 = t2; t2 = sv[2 * UPD_THREADS] - sv[3 * UPD_THREADS];
+        g1 = g2; g2 = sv[4 * UPD_THREADS];
+        tl0 = tl1; tr0 = tr1; tl1 = tl2; tr1 = tr2;
+        const int wr = rd == 0 ? UPD_SLOTS - 1 : rd - 1;           // slot of row r+1, read last iteration
+        issue(r + 2 + UPD_DEPTH, wr);
+        rd = rd == UPD_SLOTS - 1 ? 0 : rd + 1;
+    }
+    cp_async_wait<0>();
+}
+
 // ---- persistent reshaping of all cells (cell_phase_functions.cpp:461-579)
 struct ReshArgs {
     int N, z, Ntot, tpc, cap, rimax;   // tpc: strips per cell
@@ -1842,33 +1973,45 @@ __global__ void kl_copy(real *__restrict__ lum, const real *__restrict__ lumn, r
 }
 
 // The next step's centroid sums (find_centres_cells, useful_functions.cpp:
-// 193-227) over each cell's support rectangle of the reshaped phi: one warp
-// per rectangle row, exact integer sums added atomically into acc (zeroed
-// before the grid barrier that precedes this).  Nothing writes phi between
-// the end of the reshaping loops and the next step's centroids.
+// 193-227) over each cell's support rectangle of the reshaped phi: a warp
+// takes CG rows of one rectangle at once (CG loads per lane in flight per
+// column chunk), exact integer sums added atomically into acc (zeroed before
+// the grid barrier that precedes this).  Nothing writes phi between the end
+// of the reshaping loops and the next step's centroids.
 template <typename real>
 __device__ __forceinline__ void centroid_rows(const real *__restrict__ phi, const int4 *__restrict__ rect, int N,
                                               int Ntot, long long *__restrict__ acc) {
+    constexpr int CG = 4;
     const int lane = threadIdx.x & 31;
     const int nw = blockDim.x >> 5;
     const int nwt = gridDim.x * nw;
-    for (int t = blockIdx.x * nw + (threadIdx.x >> 5); t < Ntot * N; t += nwt) {
-        const int n = t / N, i = t - n * N;
+    const int groups = (N + CG - 1) / CG;
+    for (int t = blockIdx.x * nw + (threadIdx.x >> 5); t < Ntot * groups; t += nwt) {
+        const int n = t / groups, i0 = (t - n * groups) * CG;
         const int4 r = rect[n];
-        if (i < r.x || i >= r.y) continue;                       // warp-uniform
-        const real *p = phi + (size_t)n * N * N + (size_t)i * N;
-        int cnt = 0, sy = 0;                                     // at most N sites of index < N per row
-#pragma unroll 4
+        if (i0 + CG <= r.x || i0 >= r.y) continue;                 // warp-uniform
+        const real *p = phi + (size_t)n * N * N;
+        int cnt = 0, sx = 0, sy = 0;                               // < CG N sites of index < N per lane
+#pragma unroll 2
         for (int j = r.z + lane; j < r.w; j += 32) {
-            if (p[j] > (real)0.5) { cnt++; sy += j; }
+            real v[CG];
+#pragma unroll
+            for (int k = 0; k < CG; k++) {
+                const int i = i0 + k;
+                v[k] = (i >= r.x && i < r.y) ? p[(size_t)i * N + j] : (real)0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < CG; k++)
+                if (v[k] > (real)0.5) { cnt++; sx += i0 + k; sy += j; }
         }
         for (int o = 16; o > 0; o >>= 1) {
             cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+            sx += __shfl_xor_sync(0xffffffffu, sx, o);
             sy += __shfl_xor_sync(0xffffffffu, sy, o);
         }
         if (lane == 0 && cnt) {
             atomicAdd((unsigned long long *)&acc[3 * n + 0], (unsigned long long)cnt);
-            atomicAdd((unsigned long long *)&acc[3 * n + 1], (unsigned long long)((long long)cnt * i));
+            atomicAdd((unsigned long long *)&acc[3 * n + 1], (unsigned long long)sx);
             atomicAdd((unsigned long long *)&acc[3 * n + 2], (unsigned long long)sy);
         }
     }
@@ -2043,6 +2186,14 @@ struct Fused {
         r->lum_tile = (size_t)3 * (LRB + 2) * (FT + 2) * sizeof(real);
         PFAG_TRY(smem_at_least((const void *)kl_relax<real>, r->lum_tile));
         r->npsi = ((c->N + 31) / 32) * ((c->N + PT_R - 1) / PT_R);
+        r->upd_warps = 0;
+        r->upd_smem = (size_t)UPD_SLOTS * 5 * UPD_THREADS * sizeof(float);
+        if constexpr (sizeof(real) == 4) {
+            PFAG_TRY(smem_at_least((const void *)kf_update_rows<real>, r->upd_smem));
+            PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kf_update_rows<real>, UPD_THREADS,
+                                                                           r->upd_smem));
+            r->upd_warps = (long)nsm * std::max(per, 1) * (UPD_THREADS / 32);
+        }
         return PFAG_OK;
     }
 
@@ -2119,11 +2270,24 @@ struct Fused {
         cudaStream_t s = c->stream;
         if (r->fork) PFAG_CUDA_CHECK(cudaStreamWaitEvent(s, r->ev_area, 0));
         const int z = c->zone, W = 2 * z + 2;
-        dim3 gb((W + UC - 1) / UC, (W + UR - 1) / UR, c->Ntot);
         pfag_prof_begin(c, "kf_update");
-        kf_update_tiled<real><<<gb, 256, 0, s>>>(R(c->phi), R(c->phin), R(c->rho), R(c->hfunc), c->d_f0,
-                                                 R(c->psi), R(c->hlum), R(c->hecm), c->d_xc, c->d_yc, c->dp,
-                                                 R(r->Jc), R(r->G));
+        if constexpr (sizeof(real) == 4) {
+            // row chunks: as many warp tasks as fit on the GPU at once (one wave), at most
+            // one chunk per row
+            const int cg = (W + UPD_COLS - 1) / UPD_COLS;
+            const long per_chunk = (long)c->Ntot * cg;
+            const int nch = (int)std::max(1L, std::min((long)W, r->upd_warps / per_chunk));
+            const int rb = (W + nch - 1) / nch;
+            const long tasks = per_chunk * ((W + rb - 1) / rb);
+            kf_update_rows<real><<<(unsigned)((tasks + 7) / 8), UPD_THREADS, r->upd_smem, s>>>(
+                R(c->phi), R(c->phin), R(c->rho), R(c->hfunc), c->d_f0, R(c->psi), R(r->G), c->d_xc, c->d_yc, c->dp,
+                R(r->Jc), cg, (W + rb - 1) / rb, rb);
+        } else {
+            dim3 gb((W + UC - 1) / UC, (W + UR - 1) / UR, c->Ntot);
+            kf_update_tiled<real><<<gb, 256, 0, s>>>(R(c->phi), R(c->phin), R(c->rho), R(c->hfunc), c->d_f0,
+                                                     R(c->psi), R(c->hlum), R(c->hecm), c->d_xc, c->d_yc, c->dp,
+                                                     R(r->Jc), R(r->G));
+        }
         PFAG_LAUNCHED(c);
         return PFAG_OK;
     }
