@@ -275,27 +275,27 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
                                                real *__restrict__ psi, real *__restrict__ hl, real *__restrict__ he,
                                                double dx2, double *__restrict__ part_e, double *__restrict__ part_a) {
     __shared__ int list[1024];
-    __shared__ int4 lrect[1024];
-    __shared__ int2 lzone[1024];
+    __shared__ int4 lrect[1024];              // indexed by cell
+    __shared__ int2 lzone[1024];              // indexed by cell
+    __shared__ unsigned hitm[32];             // per 32-cell chunk: cells whose B_n meets the tile
     __shared__ int nlist;
     __shared__ double wq[8][32];
     const int ti0 = blockIdx.y * PT_R, tj0 = blockIdx.x * 32;
     const int tile = blockIdx.y * gridDim.x + blockIdx.x, ntiles = gridDim.x * gridDim.y;
-    if (threadIdx.x < 32) {
-        int cnt = 0;
-        for (int base = 0; base < Ntot; base += 32) {
-            const int n = base + threadIdx.x;
-            int4 r = make_int4(0, 0, 0, 0);
-            int x = 0, y = 0;
+    {
+        // every warp takes 32-cell chunks: this step's centroid (find_centres_cells)
+        // from the sums over B_n; block (0, 0) publishes it for the later
+        // kernels, every block uses its own copy (rect[n] may be old or new
+        // here: the union is the same)
+        const int nchunk = (Ntot + 31) / 32;
+        for (int ch = threadIdx.x >> 5; ch < nchunk; ch += blockDim.x >> 5) {
+            const int n = ch * 32 + (threadIdx.x & 31);
             bool hit = false;
             if (n < Ntot) {
-                // this step's centroid (find_centres_cells) from kf_centroid's sums;
-                // block (0, 0) publishes it for the later kernels, every block
-                // uses its own copy (rect[n] may be old or new here: the union is
-                // the same)
                 unsigned eb;
+                int x, y;
                 centroid_of(cacc, n, N, z, x, y, eb);
-                r = rect_with_zone(rect[n], x, y, z);
+                const int4 r = rect_with_zone(rect[n], x, y, z);
                 if (blockIdx.x == 0 && blockIdx.y == 0) {
                     if (eb) atomicOr(err, eb);
                     xc[n] = x;
@@ -303,17 +303,23 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
                     rect[n] = r;
                 }
                 hit = r.x < ti0 + PT_R && r.y > ti0 && r.z < tj0 + 32 && r.w > tj0;
+                lrect[n] = r;
+                lzone[n] = make_int2(x - z, y - z);
             }
             const unsigned m = __ballot_sync(0xffffffffu, hit);
-            if (hit) {
-                const int slot = cnt + __popc(m & ((1u << threadIdx.x) - 1u));
-                list[slot] = n;
-                lrect[slot] = r;
-                lzone[slot] = make_int2(x - z, y - z);
-            }
-            cnt += __popc(m);
+            if ((threadIdx.x & 31) == 0) hitm[ch] = m;
         }
-        if (threadIdx.x == 0) nlist = cnt;
+        __syncthreads();
+        // the tile's cells in cell order (the order of the reference's psi sum)
+        if (threadIdx.x < 32) {
+            int cnt = 0;
+            for (int ch = 0; ch < nchunk; ch++) {
+                const unsigned m = hitm[ch];
+                if ((m >> threadIdx.x) & 1u) list[cnt + __popc(m & ((1u << threadIdx.x) - 1u))] = ch * 32 + threadIdx.x;
+                cnt += __popc(m);
+            }
+            if (threadIdx.x == 0) nlist = cnt;
+        }
     }
     __syncthreads();
     const int nl = nlist;
@@ -337,8 +343,8 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
                 const bool live = u < qn;
                 const int q = q0 + (live ? u : 0);
                 const int n = list[q];
-                const int4 r = lrect[q];
-                const int zi0 = lzone[q].x, zj0 = lzone[q].y;
+                const int4 r = lrect[n];
+                const int zi0 = lzone[n].x, zj0 = lzone[n].y;
                 hp[c] = hfunc + (size_t)n * NN;
                 const real *pp = phi + (size_t)n * NN;
 #pragma unroll
@@ -1119,7 +1125,7 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) kr_boxD2(const
 }
 
 template <typename real, int M, int G, int BT>
-__global__ void __launch_bounds__(BT, 1024 / BT) kr_boxB(typename Cplx<real>::type *__restrict__ Y1,
+__global__ void __launch_bounds__(BT, 1280 / BT) kr_boxB(typename Cplx<real>::type *__restrict__ Y1,
                                                const typename Cplx<real>::type *__restrict__ Y2,
                                                const unsigned char *__restrict__ clsT, BoxArgs a) {
     typedef typename Cplx<real>::type cx;
