@@ -153,3 +153,25 @@ def test_rho_ring_after_upload_and_reupload():
     for a, b in zip(out["fused"], out["plain"]):
         for x, y in zip(a, b):
             assert rel_linf(x, y) <= 1e-9
+
+
+def test_zone_at_the_ghost_ring():
+    """A cell whose zone starts at row and column 1, so that its zone's ring
+    covers the grid's ghost row and column 0: the normals there follow the
+    periodic ghost map (useful_functions.cpp:391-420) through the fused
+    kernels' global-memory branch.  Fused FP64 against plain FP64, and the
+    FP32 areas against them, over 3 steps."""
+    from multicellular_phase_field_active_gel_organoids_b200.params import OrganoidConfig
+    cfg = OrganoidConfig("edge", 64, np.array([(18.4, 18.4), (42.0, 44.0)]), 8.0, 17, 0, 3)
+    a = run_gpu(cfg, 3, 64, capi.PATH_FUSED)
+    b = run_gpu(cfg, 3, 64, capi.PATH_PLAIN)
+    assert int(b["xc"][0]) - 17 == 1 and int(b["yc"][0]) - 17 == 1, (b["xc"], b["yc"])
+    assert np.array_equal(a["xc"], b["xc"]) and np.array_equal(a["yc"], b["yc"])
+    assert np.array_equal(a["iters"], b["iters"])
+    for k in ("phi", "rho", "lum", "ECM"):
+        assert rel_linf(a[k], b[k]) <= 1e-9, (k, rel_linf(a[k], b[k]))
+    assert rel_linf(a["s"], b["s"]) <= 1e-10
+    f = run_gpu(cfg, 3, 32, capi.PATH_FUSED)
+    assert np.array_equal(f["xc"], b["xc"])
+    assert rel_linf(f["s"], b["s"]) <= 1e-4
+    assert rel_linf(f["phi"], b["phi"]) <= 1e-3
