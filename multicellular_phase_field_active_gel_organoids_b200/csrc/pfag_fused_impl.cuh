@@ -1980,8 +1980,9 @@ __global__ void kl_copy(real *__restrict__ lum, const real *__restrict__ lumn, r
 
 // The next step's centroid sums (find_centres_cells, useful_functions.cpp:
 // 193-227) over each cell's support rectangle of the reshaped phi: a warp
-// takes CG rows of one rectangle at once (CG loads per lane in flight per
-// column chunk), exact integer sums added atomically into acc (zeroed before
+// takes CG rows of one rectangle at once (the loop over 32-column chunks is
+// unrolled by 8, so up to 8 CG loads per lane are in flight), exact integer
+// sums added atomically into acc (zeroed before
 // the grid barrier that precedes this).  Nothing writes phi between the end
 // of the reshaping loops and the next step's centroids.
 template <typename real>
@@ -1998,7 +1999,7 @@ __device__ __forceinline__ void centroid_rows(const real *__restrict__ phi, cons
         if (i0 + CG <= r.x || i0 >= r.y) continue;                 // warp-uniform
         const real *p = phi + (size_t)n * N * N;
         int cnt = 0, sx = 0, sy = 0;                               // < CG N sites of index < N per lane
-#pragma unroll 2
+#pragma unroll 8
         for (int j = r.z + lane; j < r.w; j += 32) {
             real v[CG];
 #pragma unroll
