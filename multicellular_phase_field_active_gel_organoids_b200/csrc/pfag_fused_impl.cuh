@@ -282,6 +282,15 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
     __shared__ double wq[8][32];
     const int ti0 = blockIdx.y * PT_R, tj0 = blockIdx.x * 32;
     const int tile = blockIdx.y * gridDim.x + blockIdx.x, ntiles = gridDim.x * gridDim.y;
+    // lum and ECM of this thread's sites: loaded first, used last
+    real lv[KR], ev[KR];
+#pragma unroll
+    for (int k = 0; k < KR; k++) {
+        const int i = ti0 + (threadIdx.x >> 5) + 8 * k, jj = tj0 + (threadIdx.x & 31);
+        const bool ok = i < N && jj < N;
+        lv[k] = ok ? lum[(size_t)i * N + jj] : (real)0.0;
+        ev[k] = ok ? ecm[(size_t)i * N + jj] : (real)0.0;
+    }
     {
         // every warp takes 32-cell chunks: this step's centroid (find_centres_cells)
         // from the sums over B_n; block (0, 0) publishes it for the later
@@ -389,7 +398,7 @@ __global__ void __launch_bounds__(256) kf_hpsi(const real *__restrict__ phi, rea
         if (i >= N || j >= N) continue;
         const size_t o = (size_t)i * N + j;
         psi[o] = ps[k];
-        const real a = lum[o], b = ecm[o];
+        const real a = lv[k], b = ev[k];
         hl[o] = a * a * ((real)3.0 - (real)2.0 * a);
         const real hb = b * b * ((real)3.0 - (real)2.0 * b);
         he[o] = hb;
