@@ -141,11 +141,12 @@ __device__ __forceinline__ double warp_sum_fixed(const volatile double *p, int n
     return a;
 }
 
-// Asynchronous global -> shared copy of one 4- or 8-byte element (no
-// register staging); cp_async_wait_all waits for this thread's copies.
+// Asynchronous global -> shared copy of one 4-, 8- or 16-byte element (no
+// register staging; a 16-byte one needs both addresses 16-byte aligned);
+// cp_async_wait_all waits for this thread's copies.
 template <typename T>
 __device__ __forceinline__ void cp_async_elem(T *dst, const T *src) {
-    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "element size");
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8 || sizeof(T) == 16, "element size");
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(sizeof(T)) : "memory");
 }
@@ -1502,8 +1503,27 @@ __device__ __forceinline__ double resh_tile(const real *__restrict__ P, const re
                 const int li = li0 + r - 1;                       // zone row; -1 and Z are the ring
                 const bool ring = edge_col || li < 0 || li >= Z;
                 cp_async_elem(sP + r * W + c, (ring ? pr : p) + (size_t)r * N + c);
-                cp_async_elem(sX + r * W + c, Jx + (size_t)r * W + c);
-                cp_async_elem(sY + r * W + c, Jy + (size_t)r * W + c);
+            }
+        }
+    }
+    // the normals' nr + 2 strip rows are contiguous in their W x W layout (and
+    // in the tile): 16-byte copies when every address allows them
+    {
+        typedef typename std::conditional<sizeof(real) == 4, float4, double2>::type vec;
+        constexpr int V = 16 / sizeof(real);
+        const int nJ = (nr + 2) * W;
+        const bool aligned = nJ % V == 0 &&
+                             ((reinterpret_cast<size_t>(sX) | reinterpret_cast<size_t>(sY) |
+                               reinterpret_cast<size_t>(Jx) | reinterpret_cast<size_t>(Jy)) & 15) == 0;
+        if (aligned) {
+            for (int k = threadIdx.x; k < nJ / V; k += blockDim.x) {
+                cp_async_elem(reinterpret_cast<vec *>(sX) + k, reinterpret_cast<const vec *>(Jx) + k);
+                cp_async_elem(reinterpret_cast<vec *>(sY) + k, reinterpret_cast<const vec *>(Jy) + k);
+            }
+        } else {
+            for (int k = threadIdx.x; k < nJ; k += blockDim.x) {
+                cp_async_elem(sX + k, Jx + k);
+                cp_async_elem(sY + k, Jy + k);
             }
         }
     }
@@ -1517,25 +1537,32 @@ __device__ __forceinline__ double resh_tile(const real *__restrict__ P, const re
         const size_t qo = (size_t)n * NN + (size_t)(zi0 + li0) * N + zj0 + j;
         real *q = Q + qo, *po = Pout + qo;
         const int c = j + 1;
+        // every row of the tile is computed (rows past the strip read stale tile
+        // values and are not stored), so the loads a row shares with the next
+        // one are not repeated
 #pragma unroll
         for (int r = 0; r < RB; r++) {
-            if (r < nr) {
-                const int o = (r + 1) * W + c;
-                real w[3][3];
+            const bool live = r < nr;
+            const int o = (r + 1) * W + c;
+            real w[3][3];
 #pragma unroll
-                for (int di = 0; di < 3; di++)
+            for (int di = 0; di < 3; di++)
 #pragma unroll
-                    for (int dj = 0; dj < 3; dj++) w[di][dj] = sP[o + (di - 1) * W + dj - 1];
-                const real old = w[1][1];
-                po[(size_t)r * N] = old;
-                if constexpr (sizeof(real) == 4) {
-                    const float nv = resh_update_f(kc, w, sX[o], sX[o + W], sX[o - W], sX[o + 1], sX[o - 1], sY[o],
-                                                   sY[o + W], sY[o - W], sY[o + 1], sY[o - 1], old);
+                for (int dj = 0; dj < 3; dj++) w[di][dj] = sP[o + (di - 1) * W + dj - 1];
+            const real old = w[1][1];
+            if constexpr (sizeof(real) == 4) {
+                const float nv = resh_update_f(kc, w, sX[o], sX[o + W], sX[o - W], sX[o + 1], sX[o - 1], sY[o],
+                                               sY[o + W], sY[o - W], sY[o + 1], sY[o - 1], old);
+                if (live) {
+                    po[(size_t)r * N] = old;
                     q[(size_t)r * N] = nv;
                     facc += fabsf(nv - old);
-                } else {
-                    const real nv = resh_update<real>(A, B, w, sX[o], sX[o + W], sX[o - W], sX[o + 1], sX[o - 1],
-                                                      sY[o], sY[o + W], sY[o - W], sY[o + 1], sY[o - 1], old);
+                }
+            } else {
+                const real nv = resh_update<real>(A, B, w, sX[o], sX[o + W], sX[o - W], sX[o + 1], sX[o - 1],
+                                                  sY[o], sY[o + W], sY[o - W], sY[o + 1], sY[o - 1], old);
+                if (live) {
+                    po[(size_t)r * N] = old;
                     q[(size_t)r * N] = nv;
                     acc += fabs((double)nv - (double)old) * a.scale;
                 }
