@@ -1930,28 +1930,31 @@ __global__ void __launch_bounds__(256) kl_relax(real *__restrict__ lum, real *__
     double acc = 0.0;
     float facc = 0.0f;
     if (jj < N) {
+        // every tile row holds staged (clamped) values: the stencil runs on all
+        // of them, only the stores and sums are predicated, so the loads a row
+        // shares with the next one are not repeated
 #pragma unroll
         for (int r = 0; r < LRB; r++) {
             const int ii = i0 + r;
+            const int o = (r + 1) * TW + threadIdx.x + 1;
+            real w[3][3];
+#pragma unroll
+            for (int di = 0; di < 3; di++)
+#pragma unroll
+                for (int dj = 0; dj < 3; dj++) w[di][dj] = sP[o + (di - 1) * TW + dj - 1];
+            const real old = w[1][1];
+            real nv;
+            if constexpr (sizeof(real) == 4)
+                nv = resh_update_f(kc, w, sX[o], sX[o + TW], sX[o - TW], sX[o + 1], sX[o - 1], sY[o],
+                                   sY[o + TW], sY[o - TW], sY[o + 1], sY[o - 1], old);
+            else
+                nv = resh_update<real>(A, B, w, sX[o], sX[o + TW], sX[o - TW], sX[o + 1], sX[o - 1], sY[o],
+                                       sY[o + TW], sY[o - TW], sY[o + 1], sY[o - 1], old);
             if (ii < N) {
-                const int o = (r + 1) * TW + threadIdx.x + 1;
-                const real old = sP[o];
                 real v;
                 bool edge;
                 dirichlet_val<real>(ii, jj, N, side, (real)0.0, v, edge);
-                if (!edge) {
-                    real w[3][3];
-#pragma unroll
-                    for (int di = 0; di < 3; di++)
-#pragma unroll
-                        for (int dj = 0; dj < 3; dj++) w[di][dj] = sP[o + (di - 1) * TW + dj - 1];
-                    if constexpr (sizeof(real) == 4)
-                        v = resh_update_f(kc, w, sX[o], sX[o + TW], sX[o - TW], sX[o + 1], sX[o - 1], sY[o],
-                                          sY[o + TW], sY[o - TW], sY[o + 1], sY[o - 1], old);
-                    else
-                        v = resh_update<real>(A, B, w, sX[o], sX[o + TW], sX[o - TW], sX[o + 1], sX[o - 1], sY[o],
-                                              sY[o + TW], sY[o - TW], sY[o + 1], sY[o - 1], old);
-                }
+                if (!edge) v = nv;
                 if constexpr (sizeof(real) == 4) facc += fabsf(v - old);
                 else acc += fabs((double)v - (double)old) * dx2;
                 Q[(size_t)ii * N + jj] = v;
