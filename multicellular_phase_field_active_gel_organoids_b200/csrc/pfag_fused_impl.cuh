@@ -1154,12 +1154,24 @@ __global__ void __launch_bounds__(BT, 1280 / BT) kr_boxB(typename Cplx<real>::ty
     constexpr int NZ2 = ((G + WG - 1) / WG) * WG;   // padded to whole warps
     static_assert((NSP + NZ2) % WG == 0, "slot count must be a multiple of the thread groups per warp");
     cx *Z1 = tw + M, *Z2 = Z1 + (size_t)NSP * S;
+    // the class map's columns of the block's slots (M bytes each, 16-byte
+    // aligned rows of clsT) in flight while the spectra load
+    unsigned char *scl = reinterpret_cast<unsigned char *>(Z2 + (size_t)NZ2 * S);   // [NSP][M]
+    {
+        constexpr int CH = M / 16;
+        const unsigned char *cl = clsT + (size_t)n * M * M;
+        for (int e = threadIdx.x; e < cs.ns * CH; e += BT) {
+            const int sl = e / CH, q = e - sl * CH;
+            cp_async_elem(reinterpret_cast<uint4 *>(scl + (size_t)sl * M) + q,
+                          reinterpret_cast<const uint4 *>(cl + (size_t)cs.col[sl] * M) + q);
+        }
+    }
     load_cols_fixed<cx, M, NSP, BT>(Z1, Y1 + (size_t)n * M * M, cs);
     load_cols_fixed<cx, M, NZ2, BT>(Z2, Y2 + (size_t)n * M * M, cs);
+    cp_async_wait_all();
     __syncthreads();
     columns_fft<cx, M, false>(Z1, NSP + NZ2, tw);   // Z2 follows Z1 with the same stride
     __syncthreads();
-    const unsigned char *cl = clsT + (size_t)n * M * M;
     for_pairs(cs, M, [&](int sa, int ka, int sb, int kb) {
         const cx z1a = Z1[(size_t)sa * S + ka], z1b = Z1[(size_t)sb * S + kb];
         const cx z2a = Z2[(size_t)sa * S + ka];
@@ -1174,8 +1186,8 @@ __global__ void __launch_bounds__(BT, 1280 / BT) kr_boxB(typename Cplx<real>::ty
         const int ca = cs.col[sa], cb = cs.col[sb];
         const real kxa = (real)(a.kfac * wrapk(ka, M)), kya = (real)(a.kfac * wrapk(ca, M));
         const real kxb = (real)(a.kfac * wrapk(kb, M)), kyb = (real)(a.kfac * wrapk(cb, M));
-        const real eta_a = (real)a.visc[cl[(size_t)ca * M + ka]];
-        const real eta_b = (real)a.visc[cl[(size_t)cb * M + kb]];
+        const real eta_a = (real)a.visc[scl[(size_t)sa * M + ka]];
+        const real eta_b = (real)a.visc[scl[(size_t)sb * M + kb]];
         const real fr = (real)a.friction;
         cx vxa, vya, vxb, vyb;
         velocity_at<real, cx>(kxa, kya, eta_a, fr, pxx_a, pyy_a, z2a, vxa, vya);
@@ -2515,7 +2527,7 @@ struct Fused {
         const size_t smC = (MM + (size_t)BG::ROWS * MM) * cs;
         const int nsB = 2 * GB;
         const int nz2 = ((GB + BG::WG - 1) / BG::WG) * BG::WG;
-        const size_t smB = (MM + (size_t)(nsB + nz2) * (MM + 1)) * cs;
+        const size_t smB = (MM + (size_t)(nsB + nz2) * (MM + 1)) * cs + (size_t)nsB * MM;   // + class map columns
         PFAG_TRY(smem_at_least((const void *)kr_boxA<real, MM>, smA));
         PFAG_TRY(smem_at_least((const void *)kr_boxB<real, MM, GB, 256>, smB));
         typedef BoxGeomD2<MM> BD;
