@@ -937,6 +937,28 @@ __device__ __forceinline__ void load_cols_fixed(cx *dst, const cx *__restrict__ 
     }
 }
 
+// load_cols_fixed as cp.async copies (the caller waits): all of a thread's
+// elements are in flight at once
+template <typename cx, int M, int NSP, int BT = 256>
+__device__ __forceinline__ void issue_cols_fixed(cx *dst, const cx *__restrict__ src, const ColSlots &cs) {
+    constexpr int S = M + 1, STEP = BT / NSP;
+    static_assert(NSP <= BT && (NSP & (NSP - 1)) == 0, "NSP must be a power of two <= the block size");
+    const int sl = threadIdx.x % NSP, i0 = threadIdx.x / NSP;
+    const bool live = sl < cs.ns;
+    const int col = live ? cs.col[sl] : 0;
+#pragma unroll 8
+    for (int i = i0; i < M; i += STEP) {
+        if (live) {
+            cp_async_elem(dst + (size_t)sl * S + i, src + (size_t)i * M + col);
+        } else {
+            cx v;
+            v.x = 0;
+            v.y = 0;
+            dst[(size_t)sl * S + i] = v;
+        }
+    }
+}
+
 template <typename cx, int M, int NSP, int BT = 256>
 __device__ __forceinline__ void store_cols_fixed(cx *__restrict__ dstg, const cx *src, const ColSlots &cs) {
     constexpr int S = M + 1, STEP = BT / NSP;
@@ -1056,30 +1078,21 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) kr_boxD2(const
     const int n = blockIdx.y, c0 = blockIdx.x * COLS;
     const int N = a.N;
     const real *fx = X + (size_t)n * M * M, *dy = X + (size_t)a.Ntot * M * M + (size_t)n * M * M;
-    // load column pairs: element (row i, pair p) -> Z[p][i]; U elements per
-    // thread per round, loads first
+    // load column pairs: element (row i, pair p) -> Z[p][i], the two adjacent
+    // reals of a pair as one cp.async copy (c0 + 2p is even, so it is aligned)
     constexpr int U = 4;
-    for (int e0 = threadIdx.x; e0 < NSP * M; e0 += U * blockDim.x) {
-        cx z[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const int e = e0 + u * blockDim.x;
-            const int i = e / NSP, p = e - i * NSP;
-            z[u].x = (real)0.0; z[u].y = (real)0.0;
-            if (e < NSP * M && p < NSQ) {
-                z[u].x = fx[(size_t)i * M + c0 + 2 * p];
-                z[u].y = fx[(size_t)i * M + c0 + 2 * p + 1];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const int e = e0 + u * blockDim.x;
-            if (e < NSP * M) {
-                const int i = e / NSP, p = e - i * NSP;
-                Z[(size_t)p * S + i] = z[u];
-            }
+    for (int e = threadIdx.x; e < NSP * M; e += blockDim.x) {
+        const int i = e / NSP, p = e - i * NSP;
+        if (p < NSQ) {
+            cp_async_elem(Z + (size_t)p * S + i, reinterpret_cast<const cx *>(fx + (size_t)i * M + c0 + 2 * p));
+        } else {
+            cx zz;
+            zz.x = (real)0.0;
+            zz.y = (real)0.0;
+            Z[(size_t)p * S + i] = zz;
         }
     }
+    cp_async_wait_all();
     __syncthreads();
     columns_fft<cx, M, false>(Z, NSP, tw);
     __syncthreads();
@@ -1166,8 +1179,8 @@ __global__ void __launch_bounds__(BT, 1280 / BT) kr_boxB(typename Cplx<real>::ty
                           reinterpret_cast<const uint4 *>(cl + (size_t)cs.col[sl] * M) + q);
         }
     }
-    load_cols_fixed<cx, M, NSP, BT>(Z1, Y1 + (size_t)n * M * M, cs);
-    load_cols_fixed<cx, M, NZ2, BT>(Z2, Y2 + (size_t)n * M * M, cs);
+    issue_cols_fixed<cx, M, NSP, BT>(Z1, Y1 + (size_t)n * M * M, cs);
+    issue_cols_fixed<cx, M, NZ2, BT>(Z2, Y2 + (size_t)n * M * M, cs);
     cp_async_wait_all();
     __syncthreads();
     columns_fft<cx, M, false>(Z1, NSP + NZ2, tw);   // Z2 follows Z1 with the same stride
