@@ -886,10 +886,19 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) kr_boxA(const 
 #pragma unroll
         for (int k2 = 0; k2 < TT; k2++) Y2[rowo + RF::out_index(t, r, k2)] = v[r * TT + k2];
     __syncthreads();
-    // class map transposed, ROWS consecutive bytes per column
-    for (int e = threadIdx.x; e < M * ROWS; e += blockDim.x) {
-        const int j = e / ROWS, r = e % ROWS;
-        clsT[((size_t)n * M + j) * M + i0 + r] = cls[r * (M + 4) + j];
+    // class map transposed, ROWS consecutive bytes per column, as 16-byte
+    // stores (i0 and M are multiples of 16)
+    static_assert(ROWS % 16 == 0 && M % 16 == 0, "16-byte class-map stores");
+    for (int e = threadIdx.x; e < M * (ROWS / 16); e += blockDim.x) {
+        const int j = e / (ROWS / 16), r0 = (e - j * (ROWS / 16)) * 16;
+        unsigned w[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            w[q] = 0;
+#pragma unroll
+            for (int b = 0; b < 4; b++) w[q] |= (unsigned)cls[(r0 + 4 * q + b) * (M + 4) + j] << (8 * b);
+        }
+        *reinterpret_cast<uint4 *>(clsT + ((size_t)n * M + j) * M + i0 + r0) = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
 
