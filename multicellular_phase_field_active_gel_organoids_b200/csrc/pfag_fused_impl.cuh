@@ -1780,6 +1780,9 @@ __global__ void kfl_normals(const real *__restrict__ lum, const real *__restrict
     }
 }
 
+// rows per tile of the persistent lumen / ECM iterations
+constexpr int LUM_LRI = 4;
+
 // Relaxation of the lumen and ECM fields (cell_phase_functions.cpp:774-869)
 // from iteration a.it0 on, inside the persistent kernel kf_relax_loops.
 template <typename real>
@@ -1795,7 +1798,7 @@ __device__ __forceinline__ void lum_loops(real *__restrict__ lum, real *__restri
     // left/right neighbours from the adjacent lanes.
     const real A = (real)a.A, B = (real)a.B;
     const double dx2 = a.dx * a.dx;
-    constexpr int LRI = 4;
+    constexpr int LRI = LUM_LRI;
     const int lane = threadIdx.x & 31;
     const int tiles_i = (N + LRI - 1) / LRI, tiles_j = (N + blockDim.x - 1) / blockDim.x;
     const int ntiles = tiles_i * tiles_j;
@@ -2262,6 +2265,14 @@ struct Fused {
         if (per < 1) { pfag_set_error("relaxation kernel cannot be resident with %d threads", r->resh_threads); return PFAG_E_UNSUPPORTED; }
         r->coop_r = nsm * std::min(per, 8);
         r->tpc = (2 * c->zone + RESH_RB - 1) / RESH_RB;
+        {
+            // no more blocks than the loops have tasks (reshaping strips, lumen / ECM
+            // tiles): a small organoid's persistent kernel leaves the rest of the
+            // GPU to other contexts (sweep members)
+            const long strips = (long)c->Ntot * r->tpc;
+            const long tiles = (long)((c->N + LUM_LRI - 1) / LUM_LRI) * ((c->N + r->resh_threads - 1) / r->resh_threads);
+            r->coop_r = (int)std::max(1L, std::min((long)r->coop_r, std::max(strips, tiles)));
+        }
         r->ntl = ((c->N + LRB - 1) / LRB) * ((c->N + FT - 1) / FT);
         r->lum_tile = (size_t)3 * (LRB + 2) * (FT + 2) * sizeof(real);
         PFAG_TRY(smem_at_least((const void *)kl_relax<real>, r->lum_tile));
