@@ -2363,11 +2363,11 @@ struct Fused {
         const int z = c->zone, W = 2 * z + 2;
         pfag_prof_begin(c, "kf_update");
         if constexpr (sizeof(real) == 4) {
-            // row chunks: as many warp tasks as fit on the GPU at once (one wave), at most
-            // one chunk per row
+            // row chunks: as many warp tasks as fit on the GPU at once (one wave), with at
+            // least 16 rows per task (a task loads 8 rows beyond the ones it updates)
             const int cg = (W + UPD_COLS - 1) / UPD_COLS;
             const long per_chunk = (long)c->Ntot * cg;
-            const int nch = (int)std::max(1L, std::min((long)W, r->upd_warps / per_chunk));
+            const int nch = (int)std::max(1L, std::min((long)(W + 15) / 16, r->upd_warps / per_chunk));
             const int rb = (W + nch - 1) / nch;
             const long tasks = per_chunk * ((W + rb - 1) / rb);
             kf_update_rows<real><<<(unsigned)((tasks + 7) / 8), UPD_THREADS, r->upd_smem, s>>>(
