@@ -1374,7 +1374,7 @@ __global__ void __launch_bounds__(256) kf_update_tiled(const real *__restrict__ 
 // slot is refilled one iteration after it was read.  Sites with a periodic
 // ghost neighbour (a region touching the grid's ghost ring) take their
 // normals from global memory through the ghost map.
-constexpr int UPD_COLS = 30, UPD_DEPTH = 6, UPD_SLOTS = UPD_DEPTH + 1, UPD_THREADS = 256;
+constexpr int UPD_COLS = 30, UPD_DEPTH = 4, UPD_SLOTS = UPD_DEPTH + 1, UPD_THREADS = 256;
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int K>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
