@@ -23,7 +23,7 @@ void pfag_fused_free(pfag_ctx *c) {
     if (r->side) { cudaStreamSynchronize(r->side); cudaStreamDestroy(r->side); }
     cudaEvent_t evs[] = {r->ev_psi, r->ev_area, r->ev_boxA, r->ev_lum};
     for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);
-    void *bufs[] = {r->Y1, r->Y2, r->Rb, r->clsT, r->Jc, r->Jl, r->rect, r->part_s, r->part_r, r->part_e, r->part_l,
+    void *bufs[] = {r->Y1, r->Y2, r->Rb, r->clsT, r->Jc, r->Jl, r->rect, r->part_r, r->part_e, r->part_l,
                     r->part_lt, r->part_a, r->cK, r->G};
     for (void *b : bufs) if (b) cudaFree(b);
     delete r;

@@ -57,7 +57,6 @@ inline int smem_at_least(const void *fn, size_t bytes) {
 }
 
 constexpr int FT = 256;           // threads per block of the fused kernels
-constexpr int SBLK = 32;          // blocks per cell of the support-rectangle reductions
 constexpr int RT_I = 8;            // reshaping tile: RT_I zone rows x the full zone width
 
 struct FusedRes {
@@ -67,7 +66,6 @@ struct FusedRes {
     void *Jc;               // real [Ntot][2][W][W] normals on zone + 1 ring, W = 2z+2
     void *Jl;               // real [4][N][N] lumen / ECM normals
     int4 *rect;             // [Ntot] support rectangle (i0, i1, j0, j1), half-open
-    double *part_s;         // [Ntot][SBLK]
     double *part_a;         // [Ntot][tiles^2] per-cell area partials of the psi tiles
     double *part_r;         // [Ntot][tpc]
     double *part_e;         // [npsi] sum_ecm partials
@@ -926,28 +924,11 @@ __device__ __forceinline__ void columns_fft(cx *Z, int nseq_pad, const cx *tw) {
     }
 }
 
-// Column strips: NSP (a power of two) slots of M complex each, stride M + 1.
-// Thread t always handles slot t % NSP and rows t / NSP + k * (blockDim / NSP),
-// so the loop has shift-only indexing and independent loads; slots past the
-// block's columns are zero and never stored.
-template <typename cx, int M, int NSP, int BT = 256>
-__device__ __forceinline__ void load_cols_fixed(cx *dst, const cx *__restrict__ src, const ColSlots &cs) {
-    constexpr int S = M + 1, STEP = BT / NSP;
-    static_assert(NSP <= BT && (NSP & (NSP - 1)) == 0, "NSP must be a power of two <= the block size");
-    const int sl = threadIdx.x % NSP, i0 = threadIdx.x / NSP;
-    const bool live = sl < cs.ns;
-    const int col = live ? cs.col[sl] : 0;
-#pragma unroll 8
-    for (int i = i0; i < M; i += STEP) {
-        cx v;
-        if (live) v = src[(size_t)i * M + col];
-        else { v.x = 0; v.y = 0; }
-        dst[(size_t)sl * S + i] = v;
-    }
-}
-
-// load_cols_fixed as cp.async copies (the caller waits): all of a thread's
-// elements are in flight at once
+// Column strips: NSP (a power of two) slots of M complex each, stride M + 1,
+// loaded as cp.async copies (the caller waits), so all of a thread's elements
+// are in flight at once.  Thread t always handles slot t % NSP and rows
+// t / NSP + k * (BT / NSP), so the loop has shift-only indexing; slots past
+// the block's columns are zeroed and never stored.
 template <typename cx, int M, int NSP, int BT = 256>
 __device__ __forceinline__ void issue_cols_fixed(cx *dst, const cx *__restrict__ src, const ColSlots &cs) {
     constexpr int S = M + 1, STEP = BT / NSP;
@@ -2299,7 +2280,6 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaMalloc(&r->Jl, 4 * c->ng * rs));
         if (sizeof(real) == 4) PFAG_CUDA_CHECK(cudaMalloc(&r->G, c->ng * rs));
         PFAG_CUDA_CHECK(cudaMalloc(&r->rect, sizeof(int4) * c->Ntot));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->part_s, sizeof(double) * c->Ntot * SBLK));
         {
             const size_t t = (size_t)((c->N + 31) / 32) * ((c->N + PT_R - 1) / PT_R);
             PFAG_CUDA_CHECK(cudaMalloc(&r->part_a, sizeof(double) * c->Ntot * t));
