@@ -157,8 +157,8 @@ def measured_peak_hbm():
 # FP32 path on cfg1 (profiles/fused_cfg1_f32_top_kernels.md: dram__bytes_read.sum
 # + dram__bytes_write.sum, cold caches).  Reported as roofline.traffic for that
 # workload only.
-NCU_TRAFFIC_CFG1_F32 = {"kf_boxB": 58.5e6, "kf_boxA": 107.3e6, "kf_update": 75.5e6, "kf_boxD": 70.7e6,
-                        "kf_boxC": 56.2e6, "kf_resh_first": 59.2e6, "kf_hpsi": 28.3e6, "kf_relax_loops": 19.2e6}
+NCU_TRAFFIC_CFG1_F32 = {"kf_boxB": 58.4e6, "kf_boxA": 105.0e6, "kf_update": 77.8e6, "kf_boxD": 70.1e6,
+                        "kf_boxC": 56.0e6, "kf_resh_first": 59.6e6, "kf_hpsi": 28.1e6, "kf_relax_loops": 19.2e6}
 
 
 def kernel_bytes(cfg, precision: int, iters: dict) -> dict:
