@@ -20,6 +20,7 @@ void pfag_fused_free(pfag_ctx *c) {
     FusedRes *r = F(c);
     if (!r) return;
     fused_drop_graph(r);
+    if (r->gplan_ok) cufftDestroy(r->gplan);
     if (r->side) { cudaStreamSynchronize(r->side); cudaStreamDestroy(r->side); }
     cudaEvent_t evs[] = {r->ev_psi, r->ev_area, r->ev_boxA, r->ev_lum};
     for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);

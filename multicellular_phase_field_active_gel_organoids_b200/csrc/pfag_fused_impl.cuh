@@ -74,7 +74,7 @@ struct FusedRes {
     int *cK, *cdone, *ccnt; // per cell
     int *lK, *ldone, *lcnt; // [2] lumen, ECM
     int tpc;                // reshaping strips per cell
-    int resh_threads;       // block size of the reshaping kernel (one thread per zone column)
+    int resh_threads;       // block size of the reshaping kernel (a thread per zone column, at most RESH_MAX_THREADS)
     size_t resh_smem;       // its per-warp, per-cell partial sums + strip tile
     size_t resh_tile;       // one staged strip (3 (RB+2) W reals)
     int ntl;                // lumen/ECM relaxation tiles per field (LRB rows x FT columns)
@@ -86,6 +86,9 @@ struct FusedRes {
     bool fork;
     int npsi;
     int coop_r;             // co-resident block count of the persistent kernel
+    bool generic;           // box not a power of two in 16..1024: cuFFT-based spectral passes
+    cufftHandle gplan;      // their batched 2-D transform (Ntot boxes, in place)
+    bool gplan_ok;
     long upd_warps;         // co-resident warps of kf_update_rows (FP32)
     size_t upd_smem;        // its row ring
     int logm, rows_blk, grp_cols;
@@ -771,6 +774,44 @@ __global__ void kf_boxE(const typename Cplx<real>::type *__restrict__ Y1, const 
     }
 }
 
+// One box site of the active-gel stress and reaction (compute_pi_xx/yy/xy,
+// rho_functions.cpp:32-115; create_deg_gen with compute_prod_norm_delta,
+// :193-209, :13-30; the class of create_turnover_rates_tensions, :324-353):
+// f and the central differences dxp, dyp of the cell's phi, its rho rr, and
+// lum, ECM and the index neighbours' phi at the site.  FP64 keeps the
+// reference's operation order; FP32 folds the constant factors.
+template <typename real>
+__device__ __forceinline__ void box_stress(const BoxArgs &a, real f, real dxp, real dyp, real rr, real lv, real ev,
+                                           real pm, real pp, real &xx, real &yy, real &xy, real &rt, int &c) {
+    const real c4 = (real)a.c4, sigma = (real)a.sigma;
+    const real gg = sqrt(c4 * (dxp * dxp + dyp * dyp));
+    c = map_class_f<real>(f, lv, ev, pm, pp);
+    const real at = (real)a.a_tan[c], ao = (real)a.a_ort[c], b = (real)a.bb[c];
+    xx = -at * rr * rr * rr + b * rr * rr * rr * rr;
+    yy = xx;
+    xy = (real)0.0;
+    real P;
+    if constexpr (sizeof(real) == 8) {
+        if (gg > (real)0.0) {
+            xx += (at - ao) * rr * rr * rr * c4 * dxp * dxp / gg / gg;
+            yy += (at - ao) * rr * rr * rr * c4 * dyp * dyp / gg / gg;
+            xy += (at - ao) * rr * rr * rr * c4 * dxp * dyp / gg / gg;
+        }
+        P = gg * exp(-(f - (real)0.5) * (f - (real)0.5) / (real)2.0 / sigma / sigma) / sqrt((real)(2.0 * M_PI)) /
+            sigma;
+    } else {
+        if (gg > (real)0.0) {
+            const real w = (at - ao) * rr * rr * rr * c4 / (gg * gg);
+            xx += w * dxp * dxp;
+            yy += w * dyp * dyp;
+            xy += w * dxp * dyp;
+        }
+        const real d = f - (real)0.5;
+        P = gg * (real)a.k_delta * __expf(-d * d * (real)a.inv_2s2);
+    }
+    rt = -(real)a.deg[c] * rr + (real)a.gen[c] * P;
+}
+
 // ---- box passes on register-resident FFTs (M = 32 .. 256) ----------------
 template <int M> struct BoxGeom {
     static constexpr int TT = RegFFT<float2, M>::TT;          // threads per transform
@@ -825,7 +866,6 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) kr_boxA(const 
     fft_twiddles(tw, M);
     cp_async_wait_all();
     __syncthreads();
-    const real c4 = (real)a.c4, sigma = (real)a.sigma;
     const size_t rowo = ((size_t)n * M + i) * M;
     cx v[E1];
 #pragma unroll
@@ -836,32 +876,11 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) kr_boxA(const 
         const real f = sphi[o];
         const real dxp = sphi[o + PW] - sphi[o - PW];
         const real dyp = sphi[o + 1] - sphi[o - 1];
-        const real gg = sqrt(c4 * (dxp * dxp + dyp * dyp));
-        const int c = map_class_f<real>(f, lum[s], ecm[s], phi[(size_t)n1 * NN + s], phi[(size_t)n2 * NN + s]);
-        const real rr = xys[g * M + j];
-        const real at = (real)a.a_tan[c], ao = (real)a.a_ort[c], b = (real)a.bb[c];
-        real xx = -at * rr * rr * rr + b * rr * rr * rr * rr;
-        real yy = xx, xy = (real)0.0;
-        real P;
-        if constexpr (sizeof(real) == 8) {
-            if (gg > (real)0.0) {
-                xx += (at - ao) * rr * rr * rr * c4 * dxp * dxp / gg / gg;
-                yy += (at - ao) * rr * rr * rr * c4 * dyp * dyp / gg / gg;
-                xy += (at - ao) * rr * rr * rr * c4 * dxp * dyp / gg / gg;
-            }
-            P = gg * exp(-(f - (real)0.5) * (f - (real)0.5) / (real)2.0 / sigma / sigma) / sqrt((real)(2.0 * M_PI)) /
-                sigma;
-        } else {
-            if (gg > (real)0.0) {
-                const real w = (at - ao) * rr * rr * rr * c4 / (gg * gg);
-                xx += w * dxp * dxp;
-                yy += w * dyp * dyp;
-                xy += w * dxp * dyp;
-            }
-            const real d = f - (real)0.5;
-            P = gg * (real)a.k_delta * __expf(-d * d * (real)a.inv_2s2);
-        }
-        Rb[rowo + j] = -(real)a.deg[c] * rr + (real)a.gen[c] * P;
+        real xx, yy, xy, rt;
+        int c;
+        box_stress<real>(a, f, dxp, dyp, xys[g * M + j], lum[s], ecm[s], phi[(size_t)n1 * NN + s],
+                         phi[(size_t)n2 * NN + s], xx, yy, xy, rt, c);
+        Rb[rowo + j] = rt;
         cls[g * (M + 4) + j] = (unsigned char)c;
         xys[g * M + j] = xy;
         v[q].x = xx;
@@ -1210,6 +1229,150 @@ __global__ void __launch_bounds__(BT, 1280 / BT) kr_boxB(typename Cplx<real>::ty
     store_cols_fixed<cx, M, NSP, BT>(Y1 + (size_t)n * M * M, Z1, cs);
 }
 
+// ---- spectral solve for any box size (M not a power of two, e.g. the
+//      reference's default zone_size 200, M = 398): the same steps as the
+//      register passes with cuFFT's batched 2-D transforms (5 per cell
+//      instead of the reference's 10; update_all_cortices,
+//      rho_functions.cpp:409-471).  Y1, Y2: [Ntot][M][M] complex; Rb: R;
+//      cm: the class map [Ntot][M][M] (row-major, not transposed).
+
+// stresses, reaction and class on the box: Y1 = pi_xx + i pi_yy, Y2 = pi_xy
+template <typename real>
+__global__ void kg_stress(const real *__restrict__ phi, const real *__restrict__ rho, const real *__restrict__ lum,
+                          const real *__restrict__ ecm, const int *__restrict__ xc, const int *__restrict__ yc,
+                          BoxArgs a, typename Cplx<real>::type *__restrict__ Y1,
+                          typename Cplx<real>::type *__restrict__ Y2, real *__restrict__ Rb,
+                          unsigned char *__restrict__ cm) {
+    const int n = blockIdx.y, M = a.M, N = a.N;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M * M) return;
+    const int i = e / M, j = e - i * M;
+    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
+    const int n1 = (n == 0) ? a.Ntot - 1 : n - 1, n2 = (n == a.Ntot - 1) ? 0 : n + 1;
+    const size_t NN = (size_t)N * N, s = (size_t)(bi + i) * N + (bj + j);
+    const real *p = phi + (size_t)n * NN;
+    real xx, yy, xy, rt;
+    int c;
+    box_stress<real>(a, p[s], p[s + N] - p[s - N], p[s + 1] - p[s - 1], rho[(size_t)n * NN + s], lum[s], ecm[s],
+                     phi[(size_t)n1 * NN + s], phi[(size_t)n2 * NN + s], xx, yy, xy, rt, c);
+    const size_t o = (size_t)n * M * M + e;
+    Y1[o].x = xx;
+    Y1[o].y = yy;
+    Y2[o].x = xy;
+    Y2[o].y = (real)0.0;
+    Rb[o] = rt;
+    cm[o] = (unsigned char)c;
+}
+
+// k-space velocity (update_rho_velocity, rho_functions.cpp:133-190) on each
+// pair {k, -k}: the pair's two spectra of pi_xx and pi_yy are unpacked from
+// Y1 (pi_xy is real, so its spectrum at -k is the conjugate at k), the
+// velocity at k and at -k (each with the viscosity of its own index), and the
+// Hermitian parts of vx and vy packed back as vx + i vy into Y1 at k and -k.
+template <typename real>
+__global__ void kg_velocity(typename Cplx<real>::type *__restrict__ Y1, const typename Cplx<real>::type *__restrict__ Y2,
+                            const unsigned char *__restrict__ cm, BoxArgs a) {
+    typedef typename Cplx<real>::type cx;
+    const int n = blockIdx.y, M = a.M;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M * M) return;
+    const int i = e / M, j = e - i * M;
+    const int ib = (M - i) % M, jb = (M - j) % M, eb = ib * M + jb;
+    if (eb < e) return;                      // the pair is done at its smaller index
+    cx *y1 = Y1 + (size_t)n * M * M;
+    const cx *y2 = Y2 + (size_t)n * M * M;
+    const unsigned char *cl = cm + (size_t)n * M * M;
+    const cx z1a = y1[e], z1b = y1[eb], z2a = y2[e];
+    cx z2b;
+    z2b.x = z2a.x;
+    z2b.y = -z2a.y;
+    cx pxx_a, pyy_a, pxx_b, pyy_b;
+    pxx_a.x = (real)0.5 * (z1a.x + z1b.x); pxx_a.y = (real)0.5 * (z1a.y - z1b.y);
+    pyy_a.x = (real)0.5 * (z1a.y + z1b.y); pyy_a.y = (real)0.5 * (z1b.x - z1a.x);
+    pxx_b.x = pxx_a.x; pxx_b.y = -pxx_a.y;
+    pyy_b.x = pyy_a.x; pyy_b.y = -pyy_a.y;
+    const real kxa = (real)(a.kfac * wrapk(i, M)), kya = (real)(a.kfac * wrapk(j, M));
+    const real kxb = (real)(a.kfac * wrapk(ib, M)), kyb = (real)(a.kfac * wrapk(jb, M));
+    const real fr = (real)a.friction;
+    cx vxa, vya, vxb, vyb;
+    velocity_at<real, cx>(kxa, kya, (real)a.visc[cl[e]], fr, pxx_a, pyy_a, z2a, vxa, vya);
+    velocity_at<real, cx>(kxb, kyb, (real)a.visc[cl[eb]], fr, pxx_b, pyy_b, z2b, vxb, vyb);
+    cx hx, hy;
+    hx.x = (real)0.5 * (vxa.x + vxb.x); hx.y = (real)0.5 * (vxa.y - vxb.y);
+    hy.x = (real)0.5 * (vya.x + vyb.x); hy.y = (real)0.5 * (vya.y - vyb.y);
+    cx pa, pb;
+    pa.x = hx.x - hy.y; pa.y = hx.y + hy.x;
+    pb.x = hx.x + hy.y; pb.y = hy.x - hx.y;
+    y1[e] = pa;
+    if (eb != e) y1[eb] = pb;
+}
+
+// fluxes (load_fft_rho_v, rho_functions.cpp:267-284): Y1 holds M^2 (vx + i vy);
+// Y2 = rho vx + i rho vy (and the velocity itself for debug reads)
+template <typename real>
+__global__ void kg_flux(const typename Cplx<real>::type *__restrict__ Y1, typename Cplx<real>::type *__restrict__ Y2,
+                        const real *__restrict__ rho, const int *__restrict__ xc, const int *__restrict__ yc,
+                        BoxArgs a, real *__restrict__ vdx, real *__restrict__ vdy) {
+    const int n = blockIdx.y, M = a.M, N = a.N;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M * M) return;
+    const int i = e / M, j = e - i * M;
+    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
+    const real mm = (real)((double)M * (double)M);
+    const real rr = rho[(size_t)n * N * N + (size_t)(bi + i) * N + bj + j];
+    const size_t o = (size_t)n * M * M + e;
+    const typename Cplx<real>::type v = Y1[o];
+    Y2[o].x = rr * v.x / mm;
+    Y2[o].y = rr * v.y / mm;
+    if (vdx) { vdx[o] = v.x / mm; vdy[o] = v.y / mm; }
+}
+
+// divergence term of update_fft_rho (rho_functions.cpp:213-251) on each pair
+// {k, -k}: from Y2 = FFT2(Fx + i Fy), G = -i dt kfac (ir Fx^ + jr Fy^) at k and
+// -k (ir, jr the wrapped indices, -M/2 at the Nyquist bin as the reference),
+// written over Y2
+template <typename real>
+__global__ void kg_div(typename Cplx<real>::type *__restrict__ Y2, BoxArgs a) {
+    typedef typename Cplx<real>::type cx;
+    const int n = blockIdx.y, M = a.M;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M * M) return;
+    const int i = e / M, j = e - i * M;
+    const int ib = (M - i) % M, jb = (M - j) % M, eb = ib * M + jb;
+    if (eb < e) return;
+    cx *y = Y2 + (size_t)n * M * M;
+    const cx za = y[e], zb = y[eb];
+    cx fxa, fya;                             // Fx^ and Fy^ at k; at -k their conjugates
+    fxa.x = (real)0.5 * (za.x + zb.x); fxa.y = (real)0.5 * (za.y - zb.y);
+    fya.x = (real)0.5 * (za.y + zb.y); fya.y = (real)0.5 * (zb.x - za.x);
+    const real dtk = (real)(a.dt * a.kfac);
+    const real ira = (real)wrapk(i, M), jra = (real)wrapk(j, M), irb = (real)wrapk(ib, M), jrb = (real)wrapk(jb, M);
+    cx ga, gb;
+    // -i (ir Fx + jr Fy) = (Im, -Re)
+    ga.x = dtk * (ira * fxa.y + jra * fya.y);
+    ga.y = -dtk * (ira * fxa.x + jra * fya.x);
+    gb.x = dtk * (irb * (-fxa.y) + jrb * (-fya.y));
+    gb.y = -dtk * (irb * fxa.x + jrb * fya.x);
+    y[e] = ga;
+    if (eb != e) y[eb] = gb;
+}
+
+// rho <- rho + dt R + Re(IFFT2(G)) / M^2 on the box (copy_to_rhon,
+// rho_functions.cpp:253-265, by linearity of the reference's spectral update)
+template <typename real>
+__global__ void kg_rho(const typename Cplx<real>::type *__restrict__ Y2, const real *__restrict__ Rb,
+                       real *__restrict__ rho, const int *__restrict__ xc, const int *__restrict__ yc, BoxArgs a) {
+    const int n = blockIdx.y, M = a.M, N = a.N;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M * M) return;
+    const int i = e / M, j = e - i * M;
+    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
+    const real mm = (real)((double)M * (double)M);
+    const size_t o = (size_t)n * M * M + e;
+    real &r = rho[(size_t)n * N * N + (size_t)(bi + i) * N + bj + j];
+    r = r + (real)a.dt * Rb[o] + Y2[o].x / mm;
+}
+
 // ---- phi update (cell_phase_functions.cpp:126-217) + normals
 //      (useful_functions.cpp:356-388 with the periodic ghost map of :391-420)
 // kf_update on shared-memory tiles: a block is a UR x UC tile of one cell's
@@ -1483,8 +1646,8 @@ struct ReshArgs {
 };
 
 // One reshaping strip of cell n (cell_phase_functions.cpp:486-552): zone
-// rows [strip*RB, strip*RB + RB) of Q = P + F(P), one thread per zone column
-// (blockDim >= 2z).  P's strip with its one-row, one-column ring and the
+// rows [strip*RB, strip*RB + RB) of Q = P + F(P), a thread per zone column
+// (strided by blockDim when the zone is wider than the block).  P's strip with its one-row, one-column ring and the
 // normals' strip are staged in shared memory `sm` (3 (RB+2) W reals,
 // W = 2z + 2) and the 3x3 / cross stencils read them there.  The ring, which
 // no iteration writes, comes from `Pring` (the phi update's output, whose
@@ -1547,8 +1710,7 @@ __device__ __forceinline__ double resh_tile(const real *__restrict__ P, const re
     double acc = 0.0;
     float facc = 0.0f;
     const ReshConst kc = resh_const(a.A, a.B);
-    const int j = threadIdx.x;
-    if (j < Z) {
+    for (int j = threadIdx.x; j < Z; j += blockDim.x) {       // zone columns (several per thread if Z > blockDim)
         const size_t qo = (size_t)n * NN + (size_t)(zi0 + li0) * N + zj0 + j;
         real *q = Q + qo, *po = Pout + qo;
         const int c = j + 1;
@@ -2204,13 +2366,14 @@ struct Fused {
         const int M = c->M;
         int logm = 0;
         while ((1 << logm) < M) logm++;
-        if ((1 << logm) != M || M < 16 || M > 1024) {
-            pfag_set_error("fused path needs a power-of-two FFT box (2*zone_size-2 = %d); use the plain path", M);
-            return PFAG_E_UNSUPPORTED;
-        }
+        // power-of-two boxes from 16 to 1024: the hand-written FFT passes; any
+        // other box: the cuFFT-based generic passes (kg_*)
+        r->generic = (1 << logm) != M || M < 16 || M > 1024;
+        if (M < 2) { pfag_set_error("zone_size %d gives no FFT box", c->zone); return PFAG_E_UNSUPPORTED; }
         if (c->Ntot > 1024) { pfag_set_error("fused path supports at most 1024 cells"); return PFAG_E_UNSUPPORTED; }
         r->logm = logm;
         const size_t cs = sizeof(cx);
+        if (!r->generic) {
         // rows per block for the row passes: keep the shared tile near 64 KB
         int R = std::max(1, std::min(8, (int)(65536 / (2 * (size_t)M * cs))));
         R = std::min(R, std::max(1, 8 * FT / M));   // pass C keeps <= 8 elements per thread in registers
@@ -2228,14 +2391,12 @@ struct Fused {
         PFAG_TRY(smem_at_least((const void *)kf_boxC<real>, r->smemC));
         PFAG_TRY(smem_at_least((const void *)kf_boxD<real>, r->smemD));
         PFAG_TRY(smem_at_least((const void *)kf_boxE<real>, r->smemE));
+        }
         int dev = 0, nsm = 0, per = 0;
         PFAG_CUDA_CHECK(cudaGetDevice(&dev));
         PFAG_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        r->resh_threads = 32 * ((2 * c->zone + 31) / 32);
-        if (r->resh_threads > RESH_MAX_THREADS) {
-            pfag_set_error("fused path: zone width 2*%d above %d columns; use the plain path", c->zone, RESH_MAX_THREADS);
-            return PFAG_E_UNSUPPORTED;
-        }
+        // one thread per zone column up to RESH_MAX_THREADS (wider zones: a thread takes several)
+        r->resh_threads = std::min(32 * ((2 * c->zone + 31) / 32), RESH_MAX_THREADS);
         r->resh_tile = (size_t)3 * (RESH_RB + 2) * (2 * c->zone + 2) * sizeof(real);
         r->resh_smem = (size_t)(r->resh_threads / 32) * c->Ntot * sizeof(double) + r->resh_tile;
         if (r->resh_smem > 200 * 1024) { pfag_set_error("too many cells for the reshaping kernel's per-warp sums"); return PFAG_E_UNSUPPORTED; }
@@ -2276,6 +2437,13 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaMalloc(&r->Y2, (size_t)c->Ntot * mm * 2 * rs));
         PFAG_CUDA_CHECK(cudaMalloc(&r->Rb, (size_t)c->Ntot * mm * rs));
         PFAG_CUDA_CHECK(cudaMalloc(&r->clsT, (size_t)c->Ntot * mm));
+        if (r->generic) {
+            int dims[2] = {c->M, c->M};
+            const cufftResult e = cufftPlanMany(&r->gplan, 2, dims, nullptr, 1, (int)mm, nullptr, 1, (int)mm,
+                                                sizeof(real) == 8 ? CUFFT_Z2Z : CUFFT_C2C, c->Ntot);
+            if (e != CUFFT_SUCCESS) { pfag_set_error("cufftPlanMany (%d x %d, batch %d): error %d", c->M, c->M, c->Ntot, (int)e); return PFAG_E_CUDA; }
+            r->gplan_ok = true;
+        }
         PFAG_CUDA_CHECK(cudaMalloc(&r->Jc, (size_t)c->Ntot * 2 * W * W * rs));
         PFAG_CUDA_CHECK(cudaMalloc(&r->Jl, 4 * c->ng * rs));
         if (sizeof(real) == 4) PFAG_CUDA_CHECK(cudaMalloc(&r->G, c->ng * rs));
@@ -2430,7 +2598,8 @@ struct Fused {
         const BoxArgs ba = box_args(c);
         const int Rr = r->rows_blk, G = r->grp_cols;
         cx *Y1 = (cx *)r->Y1, *Y2 = (cx *)r->Y2;
-        if (M == 256) { PFAG_TRY(box_reg<256>(ba)); }
+        if (r->generic) { PFAG_TRY(box_generic(ba)); }
+        else if (M == 256) { PFAG_TRY(box_reg<256>(ba)); }
         else if (M == 128) { PFAG_TRY(box_reg<128>(ba)); }
         else if (M == 64) { PFAG_TRY(box_reg<64>(ba)); }
         else if (M == 32) { PFAG_TRY(box_reg<32>(ba)); }
@@ -2528,6 +2697,52 @@ struct Fused {
 
     // primaries per block of the column passes (shared tile near 64 KB)
     static constexpr int GB = 4;
+
+    int fft(cx *buf, int dir) {
+        cufftResult e;
+        if constexpr (sizeof(real) == 8)
+            e = cufftExecZ2Z(r->gplan, (cufftDoubleComplex *)buf, (cufftDoubleComplex *)buf, dir);
+        else
+            e = cufftExecC2C(r->gplan, (cufftComplex *)buf, (cufftComplex *)buf, dir);
+        if (e != CUFFT_SUCCESS) { pfag_set_error("cufftExec: error %d", (int)e); return PFAG_E_CUDA; }
+        return PFAG_OK;
+    }
+
+    // spectral solve on boxes of any size: stresses, 2-D transforms of the
+    // two stress spectra, k-space velocity, inverse, fluxes, transform, the
+    // divergence multiplier, inverse, new rho on the box (the phi update runs
+    // after the stress kernel, which has read rho, lum and ECM)
+    int box_generic(const BoxArgs &ba) {
+        cudaStream_t s = c->stream;
+        const int M = c->M, Nt = c->Ntot;
+        cx *Y1 = (cx *)r->Y1, *Y2 = (cx *)r->Y2;
+        const dim3 g((M * M + 255) / 256, Nt);
+        pfag_prof_begin(c, "kf_boxA");
+        kg_stress<real><<<g, 256, 0, s>>>(R(c->phi), R(c->rho), R(c->lum), R(c->ecm), c->d_xc, c->d_yc, ba, Y1, Y2,
+                                          R(r->Rb), r->clsT);
+        PFAG_LAUNCHED(c);
+        if (r->fork) PFAG_CUDA_CHECK(cudaEventRecord(r->ev_boxA, s));
+        PFAG_TRY(launch_update());
+        if (cufftSetStream(r->gplan, s) != CUFFT_SUCCESS) { pfag_set_error("cufftSetStream failed"); return PFAG_E_CUDA; }
+        pfag_prof_begin(c, "kf_boxB");
+        PFAG_TRY(fft(Y1, CUFFT_FORWARD));
+        PFAG_TRY(fft(Y2, CUFFT_FORWARD));
+        kg_velocity<real><<<g, 256, 0, s>>>(Y1, Y2, r->clsT, ba);
+        PFAG_LAUNCHED(c);
+        PFAG_TRY(fft(Y1, CUFFT_INVERSE));
+        pfag_prof_begin(c, "kf_boxC");
+        kg_flux<real><<<g, 256, 0, s>>>(Y1, Y2, R(c->rho), c->d_xc, c->d_yc, ba, c->debug ? R(c->d_vx) : nullptr,
+                                        c->debug ? R(c->d_vy) : nullptr);
+        PFAG_LAUNCHED(c);
+        PFAG_TRY(fft(Y2, CUFFT_FORWARD));
+        pfag_prof_begin(c, "kf_boxD");
+        kg_div<real><<<g, 256, 0, s>>>(Y2, ba);
+        PFAG_LAUNCHED(c);
+        PFAG_TRY(fft(Y2, CUFFT_INVERSE));
+        kg_rho<real><<<g, 256, 0, s>>>(Y2, R(r->Rb), R(c->rho), c->d_xc, c->d_yc, ba);
+        PFAG_LAUNCHED(c);
+        return PFAG_OK;
+    }
 
     template <int MM>
     int box_reg(const BoxArgs &ba) {

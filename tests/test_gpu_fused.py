@@ -175,3 +175,41 @@ def test_zone_at_the_ghost_ring():
     assert np.array_equal(f["xc"], b["xc"])
     assert rel_linf(f["s"], b["s"]) <= 1e-4
     assert rel_linf(f["phi"], b["phi"]) <= 1e-3
+
+
+def test_box_not_a_power_of_two():
+    """zone_size 13 gives an FFT box of 24: the fused path's cuFFT-based
+    spectral passes.  Fused FP64 against plain FP64 (fields, areas, velocity)
+    over 3 steps, and the FP32 areas against them."""
+    from multicellular_phase_field_active_gel_organoids_b200.params import small_organoid
+    cfg = small_organoid(zone_size=13)
+    a = run_gpu(cfg, 3, 64, capi.PATH_FUSED, velocity=True)
+    b = run_gpu(cfg, 3, 64, capi.PATH_PLAIN, velocity=True)
+    assert np.array_equal(a["xc"], b["xc"]) and np.array_equal(a["iters"], b["iters"])
+    for k in ("phi", "rho", "lum", "ECM"):
+        assert rel_linf(a[k], b[k]) <= 1e-9, (k, rel_linf(a[k], b[k]))
+    assert rel_linf(a["s"], b["s"]) <= 1e-10
+    for va, vb in zip(a["velocity"], b["velocity"]):
+        assert rel_linf(va, vb) <= 1e-9
+    f = run_gpu(cfg, 3, 32, capi.PATH_FUSED)
+    assert np.array_equal(f["xc"], b["xc"])
+    assert rel_linf(f["s"], b["s"]) <= 1e-4
+
+
+def test_default_zone_size_200():
+    """The reference's default zone_size 200: zones 400 columns wide (a
+    reshaping thread takes several columns) and an FFT box of 398 (cuFFT-based
+    spectral passes), on a 512^2 grid with three cells.  Fused FP64 against
+    plain FP64 over 2 steps, and the FP32 areas against them."""
+    from multicellular_phase_field_active_gel_organoids_b200.params import OrganoidConfig
+    pts = np.array([(256.0, 256.0), (294.0, 256.0), (237.0, 289.0)])
+    cfg = OrganoidConfig("wide", 512, pts, 20.0, 200, 0, 2)
+    a = run_gpu(cfg, 2, 64, capi.PATH_FUSED)
+    b = run_gpu(cfg, 2, 64, capi.PATH_PLAIN)
+    assert np.array_equal(a["xc"], b["xc"]) and np.array_equal(a["iters"], b["iters"])
+    for k in ("phi", "rho", "lum", "ECM"):
+        assert rel_linf(a[k], b[k]) <= 1e-9, (k, rel_linf(a[k], b[k]))
+    assert rel_linf(a["s"], b["s"]) <= 1e-10
+    f = run_gpu(cfg, 2, 32, capi.PATH_FUSED)
+    assert np.array_equal(f["xc"], b["xc"])
+    assert rel_linf(f["s"], b["s"]) <= 1e-4
