@@ -187,5 +187,7 @@ def ring_params(N: int = 96, ncells: int = 6, radius: float = 8.0, zone_size: in
 CONFIGS = {
     "cfg0": lambda: hex_ring_organoid(),
     "cfg1": lambda: jittered_hex_organoid(),
+    # the same organoid with the reference's default zone_size (200: FFT box 398)
+    "cfg1z200": lambda: jittered_hex_organoid(name="cfg1z200", zone_size=200),
     "tiny": lambda: small_organoid(),
 }
