@@ -201,6 +201,14 @@ def kernel_bytes(cfg, precision: int, iters: dict) -> dict:
         "kfl_normals": N * N * 8 * w,
         # per launch (two launches per step): read P, Jx, Jy, write Q per active field
         "kl_relax": N * N * 4 * w * (min(lum_it, 2) + min(ecm_it, 2)) // 2,
+        # boxes that are not a power of two (cuFFT-based passes; a transform counted as one read and
+        # one write of the complex box): stresses as pass A; two forward transforms, the velocity
+        # operator (reads both spectra and the class map, writes the velocity) and one inverse;
+        # the fluxes; one forward transform, the divergence multiplier, one inverse and the new rho
+        "kg_stress": box * (6 * w + 5 * w + 1),
+        "kg_spectra": box * (3 * 4 * w + 6 * w + 1),
+        "kg_flux": box * 5 * w,
+        "kg_div": box * (3 * 4 * w + 2 * w + 3 * w),
     }
     return out
 
