@@ -21,11 +21,13 @@ void pfag_fused_free(pfag_ctx *c) {
     if (!r) return;
     fused_drop_graph(r);
     if (r->gplan_ok) cufftDestroy(r->gplan);
+    if (r->gplan_r2c_ok) cufftDestroy(r->gplan_r2c);
+    if (r->gplan_c2r_ok) cufftDestroy(r->gplan_c2r);
     if (r->side) { cudaStreamSynchronize(r->side); cudaStreamDestroy(r->side); }
     cudaEvent_t evs[] = {r->ev_psi, r->ev_area, r->ev_boxA, r->ev_lum};
     for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);
     void *bufs[] = {r->Y1, r->Y2, r->Rb, r->clsT, r->Jc, r->Jl, r->rect, r->part_r, r->part_e, r->part_l,
-                    r->part_lt, r->part_a, r->cK, r->G};
+                    r->part_lt, r->part_a, r->cK, r->G, r->Gsp};
     for (void *b : bufs) if (b) cudaFree(b);
     delete r;
     c->fused = nullptr;

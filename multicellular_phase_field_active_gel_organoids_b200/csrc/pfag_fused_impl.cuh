@@ -88,7 +88,9 @@ struct FusedRes {
     int coop_r;             // co-resident block count of the persistent kernel
     bool generic;           // box not a power of two in 16..1024: cuFFT-based spectral passes
     cufftHandle gplan;      // their batched 2-D transform (Ntot boxes, in place)
-    bool gplan_ok;
+    cufftHandle gplan_r2c, gplan_c2r;   // the fluxes' 1-D real row transforms
+    bool gplan_ok, gplan_r2c_ok, gplan_c2r_ok;
+    void *Gsp;              // the fluxes' half spectra [2][Ntot][M][M/2+1] complex
     long upd_warps;         // co-resident warps of kf_update_rows (FP32)
     size_t upd_smem;        // its row ring
     int logm, rows_blk, grp_cols;
@@ -1231,10 +1233,11 @@ __global__ void __launch_bounds__(BT, 1280 / BT) kr_boxB(typename Cplx<real>::ty
 
 // ---- spectral solve for any box size (M not a power of two, e.g. the
 //      reference's default zone_size 200, M = 398): the same steps as the
-//      register passes with cuFFT's batched 2-D transforms (5 per cell
-//      instead of the reference's 10; update_all_cortices,
-//      rho_functions.cpp:409-471).  Y1, Y2: [Ntot][M][M] complex; Rb: R;
-//      cm: the class map [Ntot][M][M] (row-major, not transposed).
+//      register passes with cuFFT's batched transforms (three 2-D ones and a
+//      1-D real pair per cell instead of the reference's ten 2-D ones;
+//      update_all_cortices, rho_functions.cpp:409-471).  Y1, Y2: [Ntot][M][M]
+//      complex (Y2 also as two real [Ntot][M][M] planes for the fluxes); Rb:
+//      R; cm: the class map [Ntot][M][M] (row-major, not transposed).
 
 // stresses, reaction and class on the box: Y1 = pi_xx + i pi_yy, Y2 = pi_xy
 template <typename real>
@@ -1307,70 +1310,87 @@ __global__ void kg_velocity(typename Cplx<real>::type *__restrict__ Y1, const ty
     if (eb != e) y1[eb] = pb;
 }
 
-// fluxes (load_fft_rho_v, rho_functions.cpp:267-284): Y1 holds M^2 (vx + i vy);
-// Y2 = rho vx + i rho vy (and the velocity itself for debug reads)
+// fluxes (load_fft_rho_v, rho_functions.cpp:267-284): Y1 holds M^2 (vx + i vy).
+// The divergence of update_fft_rho is separable (the transforms along the
+// other axis cancel): Re(IFFT2(-i ir FFT2(Fx)))/M^2 = Re(IFFT_i(-i ir FFT_i(Fx)))/M
+// along columns, likewise Fy along rows, so the fluxes go to real rows for
+// 1-D real transforms: Fr[0][n] = Fx transposed (its columns as rows),
+// Fr[1][n] = Fy.  32 x 32 tiles through shared memory keep both coalesced.
 template <typename real>
-__global__ void kg_flux(const typename Cplx<real>::type *__restrict__ Y1, typename Cplx<real>::type *__restrict__ Y2,
-                        const real *__restrict__ rho, const int *__restrict__ xc, const int *__restrict__ yc,
-                        BoxArgs a, real *__restrict__ vdx, real *__restrict__ vdy) {
-    const int n = blockIdx.y, M = a.M, N = a.N;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= M * M) return;
-    const int i = e / M, j = e - i * M;
+__global__ void __launch_bounds__(256) kg_flux(const typename Cplx<real>::type *__restrict__ Y1,
+                                               real *__restrict__ Fr, const real *__restrict__ rho,
+                                               const int *__restrict__ xc, const int *__restrict__ yc, BoxArgs a,
+                                               real *__restrict__ vdx, real *__restrict__ vdy) {
+    __shared__ real tile[32][33];
+    const int n = blockIdx.z, M = a.M, N = a.N;
+    const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
     const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
     const real mm = (real)((double)M * (double)M);
-    const real rr = rho[(size_t)n * N * N + (size_t)(bi + i) * N + bj + j];
-    const size_t o = (size_t)n * M * M + e;
-    const typename Cplx<real>::type v = Y1[o];
-    Y2[o].x = rr * v.x / mm;
-    Y2[o].y = rr * v.y / mm;
-    if (vdx) { vdx[o] = v.x / mm; vdy[o] = v.y / mm; }
+    const size_t cell = (size_t)n * M * M;
+    real *fxT = Fr + cell, *fy = Fr + (size_t)a.Ntot * M * M + cell;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = i0 + r, j = j0 + threadIdx.x;
+        if (i < M && j < M) {
+            const size_t o = (size_t)i * M + j;
+            const typename Cplx<real>::type v = Y1[cell + o];
+            const real rr = rho[(size_t)n * N * N + (size_t)(bi + i) * N + bj + j];
+            tile[r][threadIdx.x] = rr * v.x / mm;
+            fy[o] = rr * v.y / mm;
+            if (vdx) { vdx[cell + o] = v.x / mm; vdy[cell + o] = v.y / mm; }
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int j = j0 + r, i = i0 + threadIdx.x;
+        if (i < M && j < M) fxT[(size_t)j * M + i] = tile[threadIdx.x][r];
+    }
 }
 
-// divergence term of update_fft_rho (rho_functions.cpp:213-251) on each pair
-// {k, -k}: from Y2 = FFT2(Fx + i Fy), G = -i dt kfac (ir Fx^ + jr Fy^) at k and
-// -k (ir, jr the wrapped indices, -M/2 at the Nyquist bin as the reference),
-// written over Y2
+// the half spectra of the flux rows times -i k (k the row wavenumber index,
+// 0 at the Nyquist bin: the Re() of update_fft_rho's odd multiplier)
 template <typename real>
-__global__ void kg_div(typename Cplx<real>::type *__restrict__ Y2, BoxArgs a) {
-    typedef typename Cplx<real>::type cx;
-    const int n = blockIdx.y, M = a.M;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= M * M) return;
-    const int i = e / M, j = e - i * M;
-    const int ib = (M - i) % M, jb = (M - j) % M, eb = ib * M + jb;
-    if (eb < e) return;
-    cx *y = Y2 + (size_t)n * M * M;
-    const cx za = y[e], zb = y[eb];
-    cx fxa, fya;                             // Fx^ and Fy^ at k; at -k their conjugates
-    fxa.x = (real)0.5 * (za.x + zb.x); fxa.y = (real)0.5 * (za.y - zb.y);
-    fya.x = (real)0.5 * (za.y + zb.y); fya.y = (real)0.5 * (zb.x - za.x);
-    const real dtk = (real)(a.dt * a.kfac);
-    const real ira = (real)wrapk(i, M), jra = (real)wrapk(j, M), irb = (real)wrapk(ib, M), jrb = (real)wrapk(jb, M);
-    cx ga, gb;
-    // -i (ir Fx + jr Fy) = (Im, -Re)
-    ga.x = dtk * (ira * fxa.y + jra * fya.y);
-    ga.y = -dtk * (ira * fxa.x + jra * fya.x);
-    gb.x = dtk * (irb * (-fxa.y) + jrb * (-fya.y));
-    gb.y = -dtk * (irb * fxa.x + jrb * fya.x);
-    y[e] = ga;
-    if (eb != e) y[eb] = gb;
+__global__ void kg_dmul(typename Cplx<real>::type *__restrict__ S, long rows, int M) {
+    const int H = M / 2 + 1;
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= rows * H) return;
+    const int k = (int)(e % H);
+    const real kk = (real)((k == M / 2) ? 0 : k);
+    const typename Cplx<real>::type z = S[e];
+    typename Cplx<real>::type y;
+    y.x = kk * z.y;
+    y.y = -kk * z.x;
+    S[e] = y;
 }
 
-// rho <- rho + dt R + Re(IFFT2(G)) / M^2 on the box (copy_to_rhon,
-// rho_functions.cpp:253-265, by linearity of the reference's spectral update)
+// rho <- rho + dt R + dt kfac (dFx + dFy) / M on the box (copy_to_rhon,
+// rho_functions.cpp:253-265, by linearity of the reference's spectral
+// update); Fr holds M times the two derivatives, the x one transposed
 template <typename real>
-__global__ void kg_rho(const typename Cplx<real>::type *__restrict__ Y2, const real *__restrict__ Rb,
-                       real *__restrict__ rho, const int *__restrict__ xc, const int *__restrict__ yc, BoxArgs a) {
-    const int n = blockIdx.y, M = a.M, N = a.N;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= M * M) return;
-    const int i = e / M, j = e - i * M;
+__global__ void __launch_bounds__(256) kg_rho(const real *__restrict__ Fr, const real *__restrict__ Rb,
+                                              real *__restrict__ rho, const int *__restrict__ xc,
+                                              const int *__restrict__ yc, BoxArgs a) {
+    __shared__ real tile[32][33];
+    const int n = blockIdx.z, M = a.M, N = a.N;
+    const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+    const size_t cell = (size_t)n * M * M;
+    const real *dxT = Fr + cell, *dy = Fr + (size_t)a.Ntot * M * M + cell;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {            // dxT rows j0.., columns i0..
+        const int j = j0 + r, i = i0 + threadIdx.x;
+        if (i < M && j < M) tile[r][threadIdx.x] = dxT[(size_t)j * M + i];
+    }
+    __syncthreads();
     const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
-    const real mm = (real)((double)M * (double)M);
-    const size_t o = (size_t)n * M * M + e;
-    real &r = rho[(size_t)n * N * N + (size_t)(bi + i) * N + bj + j];
-    r = r + (real)a.dt * Rb[o] + Y2[o].x / mm;
+    const real dtk = (real)(a.dt * a.kfac), inv_m = (real)(1.0 / (double)M), dt = (real)a.dt;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = i0 + r, j = j0 + threadIdx.x;
+        if (i < M && j < M) {
+            const size_t o = (size_t)i * M + j;
+            real &ro = rho[(size_t)n * N * N + (size_t)(bi + i) * N + bj + j];
+            const real ti = dtk * (tile[threadIdx.x][r] * inv_m);
+            const real yy = dtk * (dy[o] * inv_m);
+            ro = ro + dt * Rb[cell + o] + (ti + yy);
+        }
+    }
 }
 
 // ---- phi update (cell_phase_functions.cpp:126-217) + normals
@@ -2439,10 +2459,20 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaMalloc(&r->clsT, (size_t)c->Ntot * mm));
         if (r->generic) {
             int dims[2] = {c->M, c->M};
-            const cufftResult e = cufftPlanMany(&r->gplan, 2, dims, nullptr, 1, (int)mm, nullptr, 1, (int)mm,
-                                                sizeof(real) == 8 ? CUFFT_Z2Z : CUFFT_C2C, c->Ntot);
+            cufftResult e = cufftPlanMany(&r->gplan, 2, dims, nullptr, 1, (int)mm, nullptr, 1, (int)mm,
+                                          sizeof(real) == 8 ? CUFFT_Z2Z : CUFFT_C2C, c->Ntot);
             if (e != CUFFT_SUCCESS) { pfag_set_error("cufftPlanMany (%d x %d, batch %d): error %d", c->M, c->M, c->Ntot, (int)e); return PFAG_E_CUDA; }
             r->gplan_ok = true;
+            // the fluxes' rows: 2 Ntot M real transforms of length M and their inverses
+            int m1 = c->M, h1 = c->M / 2 + 1;
+            const int rows = 2 * c->Ntot * c->M;
+            e = cufftPlanMany(&r->gplan_r2c, 1, &m1, &m1, 1, m1, &h1, 1, h1, sizeof(real) == 8 ? CUFFT_D2Z : CUFFT_R2C, rows);
+            if (e != CUFFT_SUCCESS) { pfag_set_error("cufftPlanMany (R2C %d, batch %d): error %d", m1, rows, (int)e); return PFAG_E_CUDA; }
+            r->gplan_r2c_ok = true;
+            e = cufftPlanMany(&r->gplan_c2r, 1, &m1, &h1, 1, h1, &m1, 1, m1, sizeof(real) == 8 ? CUFFT_Z2D : CUFFT_C2R, rows);
+            if (e != CUFFT_SUCCESS) { pfag_set_error("cufftPlanMany (C2R %d, batch %d): error %d", m1, rows, (int)e); return PFAG_E_CUDA; }
+            r->gplan_c2r_ok = true;
+            PFAG_CUDA_CHECK(cudaMalloc(&r->Gsp, (size_t)rows * h1 * 2 * rs));
         }
         PFAG_CUDA_CHECK(cudaMalloc(&r->Jc, (size_t)c->Ntot * 2 * W * W * rs));
         PFAG_CUDA_CHECK(cudaMalloc(&r->Jl, 4 * c->ng * rs));
@@ -2732,16 +2762,29 @@ struct Fused {
         c->launches++;
         PFAG_TRY(fft(Y1, CUFFT_INVERSE));
         pfag_prof_end(c);
+        real *Fr = (real *)r->Y2;              // pass B is done with Y2: the fluxes' real rows
+        const dim3 gt((M + 31) / 32, (M + 31) / 32, Nt), bt(32, 8);
         pfag_prof_begin(c, "kg_flux");
-        kg_flux<real><<<g, 256, 0, s>>>(Y1, Y2, R(c->rho), c->d_xc, c->d_yc, ba, c->debug ? R(c->d_vx) : nullptr,
+        kg_flux<real><<<gt, bt, 0, s>>>(Y1, Fr, R(c->rho), c->d_xc, c->d_yc, ba, c->debug ? R(c->d_vx) : nullptr,
                                         c->debug ? R(c->d_vy) : nullptr);
         PFAG_LAUNCHED(c);
         pfag_prof_begin(c, "kg_div");
-        PFAG_TRY(fft(Y2, CUFFT_FORWARD));
-        kg_div<real><<<g, 256, 0, s>>>(Y2, ba);
+        const long rows = 2L * Nt * M;
+        if (cufftSetStream(r->gplan_r2c, s) != CUFFT_SUCCESS || cufftSetStream(r->gplan_c2r, s) != CUFFT_SUCCESS) {
+            pfag_set_error("cufftSetStream failed");
+            return PFAG_E_CUDA;
+        }
+        cufftResult e;
+        if constexpr (sizeof(real) == 8) e = cufftExecD2Z(r->gplan_r2c, (double *)Fr, (cufftDoubleComplex *)r->Gsp);
+        else e = cufftExecR2C(r->gplan_r2c, (float *)Fr, (cufftComplex *)r->Gsp);
+        if (e != CUFFT_SUCCESS) { pfag_set_error("cufftExec (R2C): error %d", (int)e); return PFAG_E_CUDA; }
+        const long nb = rows * (M / 2 + 1);
+        kg_dmul<real><<<(unsigned)((nb + 255) / 256), 256, 0, s>>>((cx *)r->Gsp, rows, M);
         c->launches++;
-        PFAG_TRY(fft(Y2, CUFFT_INVERSE));
-        kg_rho<real><<<g, 256, 0, s>>>(Y2, R(r->Rb), R(c->rho), c->d_xc, c->d_yc, ba);
+        if constexpr (sizeof(real) == 8) e = cufftExecZ2D(r->gplan_c2r, (cufftDoubleComplex *)r->Gsp, (double *)Fr);
+        else e = cufftExecC2R(r->gplan_c2r, (cufftComplex *)r->Gsp, (float *)Fr);
+        if (e != CUFFT_SUCCESS) { pfag_set_error("cufftExec (C2R): error %d", (int)e); return PFAG_E_CUDA; }
+        kg_rho<real><<<gt, bt, 0, s>>>(Fr, R(r->Rb), R(c->rho), c->d_xc, c->d_yc, ba);
         PFAG_LAUNCHED(c);
         return PFAG_OK;
     }
