@@ -21,6 +21,7 @@ void pfag_fused_free(pfag_ctx *c) {
     if (!r) return;
     fused_drop_graph(r);
     if (r->gplan_ok) cufftDestroy(r->gplan);
+    if (r->gplan_xy_ok) cufftDestroy(r->gplan_xy);
     if (r->gplan_r2c_ok) cufftDestroy(r->gplan_r2c);
     if (r->gplan_c2r_ok) cufftDestroy(r->gplan_c2r);
     if (r->side) { cudaStreamSynchronize(r->side); cudaStreamDestroy(r->side); }

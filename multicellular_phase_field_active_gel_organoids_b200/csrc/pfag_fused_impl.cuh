@@ -88,8 +88,9 @@ struct FusedRes {
     int coop_r;             // co-resident block count of the persistent kernel
     bool generic;           // box not a power of two in 16..1024: cuFFT-based spectral passes
     cufftHandle gplan;      // their batched 2-D transform (Ntot boxes, in place)
+    cufftHandle gplan_xy;   // pi_xy's real 2-D transform
     cufftHandle gplan_r2c, gplan_c2r;   // the fluxes' 1-D real row transforms
-    bool gplan_ok, gplan_r2c_ok, gplan_c2r_ok;
+    bool gplan_ok, gplan_xy_ok, gplan_r2c_ok, gplan_c2r_ok;
     void *Gsp;              // the fluxes' half spectra [2][Ntot][M][M/2+1] complex
     long upd_warps;         // co-resident warps of kf_update_rows (FP32)
     size_t upd_smem;        // its row ring
@@ -1239,7 +1240,7 @@ __global__ void __launch_bounds__(BT, 1280 / BT) kr_boxB(typename Cplx<real>::ty
 //      complex (Y2 also as two real [Ntot][M][M] planes for the fluxes); Rb:
 //      R; cm: the class map [Ntot][M][M] (row-major, not transposed).
 
-// stresses, reaction and class on the box: Y1 = pi_xx + i pi_yy, Y2 = pi_xy
+// stresses, reaction and class on the box: Y1 = pi_xx + i pi_yy, Y2 (as reals) = pi_xy
 template <typename real>
 __global__ void kg_stress(const real *__restrict__ phi, const real *__restrict__ rho, const real *__restrict__ lum,
                           const real *__restrict__ ecm, const int *__restrict__ xc, const int *__restrict__ yc,
@@ -1261,19 +1262,19 @@ __global__ void kg_stress(const real *__restrict__ phi, const real *__restrict__
     const size_t o = (size_t)n * M * M + e;
     Y1[o].x = xx;
     Y1[o].y = yy;
-    Y2[o].x = xy;
-    Y2[o].y = (real)0.0;
+    reinterpret_cast<real *>(Y2)[o] = xy;   // a real plane, for a real-to-complex transform
     Rb[o] = rt;
     cm[o] = (unsigned char)c;
 }
 
 // k-space velocity (update_rho_velocity, rho_functions.cpp:133-190) on each
 // pair {k, -k}: the pair's two spectra of pi_xx and pi_yy are unpacked from
-// Y1 (pi_xy is real, so its spectrum at -k is the conjugate at k), the
+// Y1, pi_xy's from its half spectrum (it is real, so its spectrum at -k is the
+// conjugate at k), the
 // velocity at k and at -k (each with the viscosity of its own index), and the
 // Hermitian parts of vx and vy packed back as vx + i vy into Y1 at k and -k.
 template <typename real>
-__global__ void kg_velocity(typename Cplx<real>::type *__restrict__ Y1, const typename Cplx<real>::type *__restrict__ Y2,
+__global__ void kg_velocity(typename Cplx<real>::type *__restrict__ Y1, const typename Cplx<real>::type *__restrict__ Hxy,
                             const unsigned char *__restrict__ cm, BoxArgs a) {
     typedef typename Cplx<real>::type cx;
     const int n = blockIdx.y, M = a.M;
@@ -1283,10 +1284,17 @@ __global__ void kg_velocity(typename Cplx<real>::type *__restrict__ Y1, const ty
     const int ib = (M - i) % M, jb = (M - j) % M, eb = ib * M + jb;
     if (eb < e) return;                      // the pair is done at its smaller index
     cx *y1 = Y1 + (size_t)n * M * M;
-    const cx *y2 = Y2 + (size_t)n * M * M;
+    const int H = M / 2 + 1;
+    const cx *h = Hxy + (size_t)n * M * H;  // pi_xy's half spectrum [M][M/2+1]
     const unsigned char *cl = cm + (size_t)n * M * M;
-    const cx z1a = y1[e], z1b = y1[eb], z2a = y2[e];
-    cx z2b;
+    const cx z1a = y1[e], z1b = y1[eb];
+    cx z2a, z2b;                             // pi_xy^ at k and at -k (its conjugate)
+    if (j < H) {
+        z2a = h[(size_t)i * H + j];
+    } else {
+        z2a = h[(size_t)ib * H + jb];
+        z2a.y = -z2a.y;
+    }
     z2b.x = z2a.x;
     z2b.y = -z2a.y;
     cx pxx_a, pyy_a, pxx_b, pyy_b;
@@ -2463,6 +2471,12 @@ struct Fused {
                                           sizeof(real) == 8 ? CUFFT_Z2Z : CUFFT_C2C, c->Ntot);
             if (e != CUFFT_SUCCESS) { pfag_set_error("cufftPlanMany (%d x %d, batch %d): error %d", c->M, c->M, c->Ntot, (int)e); return PFAG_E_CUDA; }
             r->gplan_ok = true;
+            // pi_xy: Ntot real 2-D transforms (half spectra into Gsp)
+            int hdims[2] = {c->M, c->M / 2 + 1};
+            e = cufftPlanMany(&r->gplan_xy, 2, dims, dims, 1, (int)mm, hdims, 1, c->M * (c->M / 2 + 1),
+                              sizeof(real) == 8 ? CUFFT_D2Z : CUFFT_R2C, c->Ntot);
+            if (e != CUFFT_SUCCESS) { pfag_set_error("cufftPlanMany (R2C %d x %d, batch %d): error %d", c->M, c->M, c->Ntot, (int)e); return PFAG_E_CUDA; }
+            r->gplan_xy_ok = true;
             // the fluxes' rows: 2 Ntot M real transforms of length M and their inverses
             int m1 = c->M, h1 = c->M / 2 + 1;
             const int rows = 2 * c->Ntot * c->M;
@@ -2757,8 +2771,14 @@ struct Fused {
         // profiled segments: the transforms count with the kernel between them
         pfag_prof_begin(c, "kg_spectra");
         PFAG_TRY(fft(Y1, CUFFT_FORWARD));
-        PFAG_TRY(fft(Y2, CUFFT_FORWARD));
-        kg_velocity<real><<<g, 256, 0, s>>>(Y1, Y2, r->clsT, ba);
+        {
+            if (cufftSetStream(r->gplan_xy, s) != CUFFT_SUCCESS) { pfag_set_error("cufftSetStream failed"); return PFAG_E_CUDA; }
+            cufftResult e;
+            if constexpr (sizeof(real) == 8) e = cufftExecD2Z(r->gplan_xy, (double *)Y2, (cufftDoubleComplex *)r->Gsp);
+            else e = cufftExecR2C(r->gplan_xy, (float *)Y2, (cufftComplex *)r->Gsp);
+            if (e != CUFFT_SUCCESS) { pfag_set_error("cufftExec (R2C 2-D): error %d", (int)e); return PFAG_E_CUDA; }
+        }
+        kg_velocity<real><<<g, 256, 0, s>>>(Y1, (const cx *)r->Gsp, r->clsT, ba);
         c->launches++;
         PFAG_TRY(fft(Y1, CUFFT_INVERSE));
         pfag_prof_end(c);
