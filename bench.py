@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--config", default="cfg1")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
+    ap.add_argument("--members", type=int, default=256, help="cfg3: organoids in the batched sweep")
+    ap.add_argument("--no-tune", action="store_true", help="cfg3: default launch shapes (no autotuning)")
     return ap.parse_args()
 
 
@@ -153,17 +155,39 @@ def measured_peak_hbm():
 
 
 # ---------------------------------------------------------------------------
-# DRAM bytes (read + write) of one launch, from one ncu capture of the fused
-# FP32 path on cfg1 (profiles/fused_cfg1_f32_top_kernels.md: dram__bytes_read.sum
-# + dram__bytes_write.sum, cold caches).  Reported as roofline.traffic for that
-# workload only.
-NCU_TRAFFIC_CFG1_F32 = {"kf_boxB": 58.4e6, "kf_boxA": 105.0e6, "kf_update": 77.8e6, "kf_boxD": 70.1e6,
-                        "kf_boxC": 56.0e6, "kf_resh_first": 59.6e6, "kf_hpsi": 28.1e6, "kf_relax_loops": 19.2e6}
+# DRAM bytes (read + write) of one launch of the dominant kernel, from the
+# committed ncu captures (dram__bytes_read.sum + dram__bytes_write.sum, one cold
+# launch) of the fused FP32 step: (config, kernel) -> (bytes, profile file).
+NCU_TRAFFIC = {
+    ("cfg1", "kr_boxB"): (58.4e6, "profiles/fused_cfg1_f32_top_kernels.md"),
+    ("cfg1", "kr_boxA"): (105.0e6, "profiles/fused_cfg1_f32_top_kernels.md"),
+    ("cfg1", "kf_update_rows"): (77.8e6, "profiles/fused_cfg1_f32_top_kernels.md"),
+    ("cfg1", "kr_boxD2"): (70.1e6, "profiles/fused_cfg1_f32_top_kernels.md"),
+    ("cfg1", "kr_boxC2"): (56.0e6, "profiles/fused_cfg1_f32_top_kernels.md"),
+    ("cfg1", "kf_resh_first"): (59.6e6, "profiles/fused_cfg1_f32_top_kernels.md"),
+}
 
 
-def kernel_bytes(cfg, precision: int, iters: dict) -> dict:
-    """Algorithmic bytes per launch of the fused kernels (compulsory traffic:
-    each array element the kernel must read or write once)."""
+def footprints(cfg, xc, yc):
+    """Sites of the union over cells of the FFT boxes and of the zone + ring
+    regions (the parts of a shared [N][N] array the box and update passes touch)."""
+    N, z, M = cfg.N, cfg.zone_size, cfg.box
+    ub = np.zeros((N, N), bool)
+    ur = np.zeros((N, N), bool)
+    for i, j in zip(np.asarray(xc), np.asarray(yc)):
+        ub[max(i - z + 1, 0):i - z + 1 + M, max(j - z + 1, 0):j - z + 1 + M] = True
+        ur[max(i - z - 1, 0):i + z + 1, max(j - z - 1, 0):j + z + 1] = True
+    return int(ub.sum()), int(ur.sum())
+
+
+def kernel_bytes(cfg, precision: int, iters: dict, ubox: int, uring: int) -> dict:
+    """Algorithmic bytes per launch of the fused kernels: every array element
+    the launch must read or write, each counted once per launch.  A per-cell
+    array counts over the cells' boxes (box = Ntot M^2 sites), zones
+    (zone = Ntot (2z)^2) or zone + ring regions (ring = Ntot (2z+2)^2); a
+    neighbour cell's phi read on a cell's box is the same array and is not
+    counted again; a shared [N][N] array counts once over the union of the
+    regions the launch touches (ubox, uring sites) or over the grid."""
     w = precision // 8
     n, N, z = cfg.ncells, cfg.N, cfg.zone_size
     M, Wz = cfg.box, 2 * z + 2
@@ -174,16 +198,20 @@ def kernel_bytes(cfg, precision: int, iters: dict) -> dict:
     ecm_it = max(iters.get("ecm_iters", 1), 1)
     cell_it = max(iters.get("cell_iters_sum", n), n)
     out = {
-        # reads phi (centre), phi_{n-1}, phi_{n+1}, rho, lum, ECM; writes pi_xx+i pi_yy, pi_xy, R, class byte
-        "kf_boxA": box * (6 * w + 5 * w + 1),
-        "kf_boxB": box * (4 * w + 1 + 2 * w),
-        # reads Y1 (complex), rho; writes Fx and the row term
-        "kf_boxC": box * (2 * w + w + 2 * w),
+        # reads phi, rho (per cell), lum, ECM (shared); writes pi_xx + i pi_yy, pi_xy (complex),
+        # R and the class byte
+        "kr_boxA": box * (2 * w + 2 * w + 2 * w + w + 1) + ubox * 2 * w,
+        # reads the two row spectra (pi_xy's primary columns only: half of it) and the class map;
+        # writes the packed velocity spectrum
+        "kr_boxB": box * (2 * w + w + 1 + 2 * w),
+        # reads the velocity spectrum and rho; writes Fx and the row term
+        "kr_boxC2": box * (2 * w + w + 2 * w),
         # reads Fx, the row term, rho, R; writes rho in place
-        "kf_boxD": box * 5 * w,
-        # reads phi, rho, hfunc, psi and (FP64) h(lum), h(ECM) or (FP32) the coupling term G;
-        # writes phin, J_x, J_y
-        "kf_update": ring * (9 if precision == 64 else 8) * w,
+        "kr_boxD2": box * 5 * w,
+        # reads phi, rho, hfunc (per cell), psi and the coupling term G (shared); writes phin, J_x, J_y
+        "kf_update_rows": ring * 6 * w + uring * 2 * w,
+        # reads phi, rho, hfunc (per cell), psi, h(lum), h(ECM) (shared); writes phin, J_x, J_y
+        "kf_update_tiled": ring * 6 * w + uring * 3 * w,
         # FP32: reads h(lum), h(ECM), writes G
         "kf_gel_coupling": N * N * 3 * w,
         # reshaping iteration 1: read P and J (x, y), write Q and phi (P), over every zone
@@ -201,16 +229,32 @@ def kernel_bytes(cfg, precision: int, iters: dict) -> dict:
         "kfl_normals": N * N * 8 * w,
         # per launch (two launches per step): read P, Jx, Jy, write Q per active field
         "kl_relax": N * N * 4 * w * (min(lum_it, 2) + min(ecm_it, 2)) // 2,
-        # boxes that are not a power of two (cuFFT-based passes; a transform counted as one read and
-        # one write of the complex box): stresses as pass A; two forward transforms, the velocity
-        # operator (reads both spectra and the class map, writes the velocity) and one inverse;
-        # the fluxes; one forward transform, the divergence multiplier, one inverse and the new rho
-        "kg_stress": box * (6 * w + 5 * w + 1),
-        "kg_spectra": box * (3 * 4 * w + 6 * w + 1),
-        "kg_flux": box * 5 * w,
-        "kg_div": box * (3 * 4 * w + 2 * w + 3 * w),
+        # boxes that are not a power of two (Bluestein passes)
+        # stresses: reads phi, rho (per cell), lum, ECM (shared); writes Y1 (complex), pi_xy (real), R, class
+        "kg_stress": box * (2 * w + 2 * w + w + w + 1) + ubox * 2 * w,
+        # rows: reads Y1 (complex) and pi_xy (real); writes Y1 and pi_xy's half spectra
+        "kbl_rowsA": box * (2 * w + w + 2 * w + w),
+        # columns: Y1 read and written, pi_xy's half spectra read and written
+        "kbl_colsB": box * (4 * w + 2 * w),
+        # reads both spectra (pi_xy's half) and the class map, writes the velocity spectrum
+        "kg_velocity": box * (2 * w + w + 1 + 2 * w),
+        # inverse columns: Y1 read and written
+        "kbl_colsC": box * 4 * w,
+        # inverse rows: reads Y1 and rho; writes Fx and the row term
+        "kbl_rowsD": box * (2 * w + w + 2 * w),
+        # column derivative and the new rho: reads Fx, the row term, R, rho; writes rho
+        "kbl_colsE": box * 5 * w,
     }
     return out
+
+
+def step_bytes(cfg, precision: int) -> int:
+    """Compulsory state traffic of one step: per cell, phi and rho read and
+    written over the zone; the shared psi, lumen and ECM read and written
+    (B_step = Ntot Z 4w + N^2 6w, Z = (2 zone_size)^2)."""
+    w = precision // 8
+    Z = (2 * cfg.zone_size) ** 2
+    return cfg.ncells * Z * 4 * w + cfg.N * cfg.N * 6 * w
 
 
 def run_ours(args, ws, rank, local, dist: Dist):
@@ -307,23 +351,34 @@ def run_ours(args, ws, rank, local, dist: Dist):
     # roofline of the dominant kernel
     iters_per_step = {"cell_iters_sum": stats["cell_iters_sum"], "lum_iters": stats["lum_iters"],
                       "ecm_iters": stats["ecm_iters"]}
-    kb = kernel_bytes(cfg, prec, iters_per_step)
+    xc, yc = sim.centres()
+    ubox, uring = footprints(cfg, xc, yc)
+    kb = kernel_bytes(cfg, prec, iters_per_step, ubox, uring)
     top = max(ktimes.items(), key=lambda kv: kv[1][0]) if ktimes else ("none", (0.0, 1))
     top_name, (top_ms, top_launches) = top
     peak, peak_kind = measured_peak_hbm()
     per_launch_ms = top_ms / max(top_launches, 1)
     achieved = kb.get(top_name, 0) / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
     total_k_ms = sum(v[0] for v in ktimes.values()) or 1.0
+    traffic = NCU_TRAFFIC.get((args.config, top_name)) if prec == 32 else None
+    b_step = step_bytes(cfg, prec)
+    step_ms = float(np.mean(ms))
+    step_gbs = b_step / (step_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": top_name, "achieved": round(achieved, 1), "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": (NCU_TRAFFIC_CFG1_F32.get(top_name)
-                            if args.config == "cfg1" and prec == 32 else None),
-                "traffic_source": "ncu capture, profiles/fused_cfg1_f32_top_kernels.md",
+                "algorithmic_bytes_per_launch": int(kb.get(top_name, 0)),
+                "launch_ms": round(per_launch_ms, 5),
+                "traffic": traffic[0] if traffic else None,
+                "traffic_source": traffic[1] if traffic else None,
                 "share": round(top_ms / total_k_ms, 3),
+                "step_bytes": int(b_step), "step_achieved": round(step_gbs, 1),
+                "step_frac": round(step_gbs / peak, 4),
                 "timing": f"per-launch CUDA events over {nprof} eager profiled steps after the timed region",
                 "per_kernel_ms_per_step": {k: round(v[0] / nprof, 4) for k, v in sorted(ktimes.items())},
                 "per_kernel_gbs": {k: round(kb[k] / (v[0] / max(v[1], 1) * 1e-3) / 1e9, 1)
-                                   for k, v in ktimes.items() if k in kb and v[0] > 0}}
+                                   for k, v in ktimes.items() if k in kb and v[0] > 0},
+                "per_kernel_frac": {k: round(kb[k] / (v[0] / max(v[1], 1) * 1e-3) / 1e9 / peak, 3)
+                                    for k, v in ktimes.items() if k in kb and v[0] > 0}}
     sim.close()
 
     # end to end through the public C ABI: pinned host buffers in, K steps, state out
@@ -405,6 +460,110 @@ def compare_paths(cfg, p, capi, nsteps=20):
     return out
 
 
+def run_batched(args, ws, rank, local, dist: Dist):
+    """Config 3: the seeded uneven sweep (members generated on the device),
+    one graph launch per step over every member; each GPU its own replica."""
+    from multicellular_phase_field_active_gel_organoids_b200 import batched as B
+    from multicellular_phase_field_active_gel_organoids_b200 import capi
+
+    capi.lib()
+    rt = ctypes.CDLL("libcudart.so.12")
+    if rt.cudaSetDevice(local) != 0:
+        raise RuntimeError(f"cudaSetDevice({local}) failed")
+    rt.cudaEventCreate.argtypes = [ctypes.POINTER(ctypes.c_void_p)]
+    rt.cudaEventRecord.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    rt.cudaEventElapsedTime.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_void_p, ctypes.c_void_p]
+    rt.cudaMemsetAsync.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p]
+    rt.cudaStreamSynchronize.argtypes = [ctypes.c_void_p]
+    prec = args.precision
+    members = B.sweep_members(args.members, seed=1)
+    t0 = time.perf_counter()
+    shapes = {} if args.no_tune else B.autotune(members, prec)
+    t_tune = time.perf_counter() - t0
+    sw = B.BatchedSweep(members, prec)
+    sw.set_shapes(shapes)
+    sites = sw.sites
+    flush = ctypes.c_void_p()
+    assert rt.cudaMalloc(ctypes.byref(flush), ctypes.c_size_t(L2_FLUSH_BYTES)) == 0
+    stream = ctypes.c_void_p(sw.batch.stream())
+    it = 0
+    for _ in range(max(args.warmup, 3)):
+        sw.step(it, 1)
+        it += 1
+    nev = args.steps
+    ev0 = [ctypes.c_void_p() for _ in range(nev)]
+    ev1 = [ctypes.c_void_p() for _ in range(nev)]
+    for e in ev0 + ev1:
+        rt.cudaEventCreate(ctypes.byref(e))
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    dist.barrier()
+    rt.cudaStreamSynchronize(stream)
+    launches = 0
+    for k in range(nev):
+        rt.cudaMemsetAsync(flush, k & 0xff, L2_FLUSH_BYTES, stream)
+        rt.cudaEventRecord(ev0[k], stream)
+        sw.step_async(it, 1)
+        launches += sw.batch.launch_count()
+        rt.cudaEventRecord(ev1[k], stream)
+        it += 1
+    rt.cudaStreamSynchronize(stream)
+    dist.barrier()
+    clocks = sampler.stop()
+    sw.sync()
+    ms = []
+    for k in range(nev):
+        f = ctypes.c_float()
+        rt.cudaEventElapsedTime(ctypes.byref(f), ev0[k], ev1[k])
+        ms.append(f.value)
+    total_ms = dist.max(float(np.sum(ms)))
+    value = sites * nev * ws / (total_ms * 1e-3)
+    # step-level roofline: the members' compulsory state bytes per step
+    peak, peak_kind = measured_peak_hbm()
+    b_step = sum(step_bytes(m.config(), prec) for m in sw.members)
+    step_ms = float(np.mean(ms))
+    step_gbs = b_step / (step_ms * 1e-3) / 1e9
+    # end to end through the public batch API: every step's areas, f0 and
+    # centres of every member copied to pinned host rows
+    obs = [(np.empty(m.ncells), np.empty(m.ncells), np.empty(m.ncells, np.int32), np.empty(m.ncells, np.int32))
+           for m in sw.members]
+    rt.cudaHostRegister.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint]
+    rt.cudaHostUnregister.argtypes = [ctypes.c_void_p]
+    for row in obs:
+        for a in row:
+            rt.cudaHostRegister(a.ctypes.data, a.nbytes, 0)
+    L = capi.lib()
+    dist.barrier()
+    te0 = time.perf_counter()
+    for k in range(nev):
+        sw.step_async(it, 1)
+        it += 1
+        for s, row in zip(sw.sims, obs):
+            capi.check(L.pfag_observables_async(s.h, *[ctypes.c_void_p(a.ctypes.data) for a in row]))
+    sw.sync()
+    te = dist.max(time.perf_counter() - te0)
+    for row in obs:
+        for a in row:
+            rt.cudaHostUnregister(a.ctypes.data)
+    d2h = sum(a.nbytes for row in obs for a in row)
+    e2e = {"value": sites * nev * ws / te, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(d2h),
+           "steps": nev, "note": "pfag_batch_step_async per step (one graph launch over every member) with every "
+                                 "member's areas, f0 and centres copied to pinned host rows; member states are "
+                                 "generated on the device (pfag_seed_organoid), so no state crosses PCIe"}
+    buckets = {k: len(v) for k, v in sw.buckets().items()}
+    sw.close()
+    rt.cudaFree(flush)
+    return {"value": value, "ms_per_step": dist.max(step_ms), "e2e": e2e, "clocks": clocks,
+            "gpu_launches": int(dist.sum(launches)), "sites": sites, "members": len(members),
+            "roofline": {"bound": "hbm", "kernel": None, "achieved": round(step_gbs, 1), "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(step_gbs / peak, 4), "traffic": None,
+                         "step_bytes": int(b_step), "step_achieved": round(step_gbs, 1),
+                         "step_frac": round(step_gbs / peak, 4),
+                         "note": "step level: the members' compulsory state bytes per step over the batch step time"},
+            "tuning": {"seconds": round(t_tune, 1), "shapes": shapes, "buckets": buckets}}
+
+
 def cpu_reference_rate(cfg_name: str, steps: int, warmup: int, precision: str = "fp32"):
     """The reference's own step (oracle/_ref, g++ build, serial) on the host."""
     from multicellular_phase_field_active_gel_organoids_b200.params import CONFIGS
@@ -438,6 +597,8 @@ def main():
     args = parse()
     ws, rank, local = dist_info()
     from multicellular_phase_field_active_gel_organoids_b200.params import CONFIGS
+    if args.config == "cfg3":
+        return main_batched(args, ws, rank, local)
     cfg = CONFIGS[args.config]()
     config = {"workload": f"{args.config}: {cfg.N}x{cfg.N} periodic grid, {cfg.ncells} cells R={cfg.radius:g} "
                           f"on a jittered hexagonal lattice, zone_size {cfg.zone_size} (FFT box {cfg.box}), "
@@ -456,7 +617,8 @@ def main():
                 "ms_per_step": el / k * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic (seeded organoid, same generator as our arm)", "config": config,
                 "impl": "reference",
-                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
+                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "reference",
+                                 "host_cores": os.cpu_count(), "sample": sample},
                 "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0
@@ -468,8 +630,9 @@ def main():
         try:
             r = cpu_reference_rate(args.config, 2, 1, "fp32")
             if r:
-                cpu = {"value": r[0], "unit": UNIT, "cores": 1, "kind": "reference",
-                       "sample": "2 steps (after 1 warm-up) of the full workload, reference FP32 build, 1 core"}
+                cpu = {"value": r[0], "unit": UNIT, "cores": 1, "kind": "reference", "host_cores": os.cpu_count(),
+                       "sample": "2 steps (after 1 warm-up) of the full workload, reference FP32 build, 1 core "
+                                 "(the reference's host code is serial without OpenACC)"}
         except Exception as e:  # pragma: no cover - reported, not fatal
             cpu = {"error": str(e)[:200]}
     dist.close()
@@ -489,6 +652,72 @@ def main():
             "relax_iters_last_step": res["stats"]}
     if "compare" in res:
         line["compare_vs_plain_f64"] = res["compare"]
+    print(json.dumps(line))
+    return 0
+
+
+def main_batched(args, ws, rank, local):
+    config = {"workload": f"cfg3: batched uneven sweep of {args.members} seeded organoids (seed 1): grids 256^2, "
+                          "512^2 or 1024^2, cell counts log-uniform in [8, 128] capped by the grid, radii U(16, 32), "
+                          "FFT boxes 4R rounded up to a multiple of 16 (64..128), contractility and turnover x "
+                          "U(0.5, 2); one graph launch per step over every member",
+              "members": args.members, "l2": "flushed between timed steps (256 MiB write)", "replicas": ws,
+              "path": "fused", "precision": "f32 with f64 areas/loop sums" if args.precision == 32 else "f64",
+              "parallelism": f"replicas x{ws}"}
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        # the reference's own step on the host for a bounded sample: the first
+        # 256^2 members of the same sweep, one step each
+        from multicellular_phase_field_active_gel_organoids_b200 import batched as B
+        from oracle import refrun
+        ms = [m for m in B.sweep_members(args.members, seed=1) if m.N == 256][:4]
+        el = 0.0
+        sites = 0
+        for m in ms:
+            code = f"""
+import sys, time, json, numpy as np
+sys.path.insert(0, {ROOT!r})
+from multicellular_phase_field_active_gel_organoids_b200 import batched as B
+from oracle.refrun import RefLib
+m = [x for x in B.sweep_members({args.members}, seed=1) if x.index == {m.index}][0]
+cfg = m.config()
+r = RefLib('fp32', cfg.params())
+r.load(*cfg.initial_state(np.float32))
+r.step(0)
+t = time.perf_counter()
+r.step(1)
+print('RESULT', json.dumps({{'el': time.perf_counter() - t}}))
+"""
+            out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=1800)
+            line = [l for l in out.stdout.splitlines() if l.startswith("RESULT")]
+            if not line:
+                raise RuntimeError("reference run failed: " + out.stderr[-2000:])
+            el += json.loads(line[0].split(" ", 1)[1])["el"]
+            sites += m.sites
+        rate = sites / el
+        line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": 1, "warmup": 1,
+                "ms_per_step": el * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic (seeded sweep members, same generator as our arm)",
+                "config": config, "impl": "reference",
+                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "reference",
+                                 "host_cores": os.cpu_count(),
+                                 "sample": f"one step (after one warm-up step) of each of the first {len(ms)} "
+                                           "256^2 members, shipped FP32 build, one process"},
+                "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+    dist = Dist(ws, rank, local, "nccl")
+    res = run_batched(args, ws, rank, local, dist)
+    dist.close()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": res["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == 32 else "f64",
+            "data": "synthetic (seeded organoids generated on the device; no dataset)",
+            "config": dict(config, sites_per_step=res["sites"]), "roofline": res["roofline"], "cpu_baseline": None,
+            "e2e": res["e2e"], "gpu_launches": res["gpu_launches"], "clocks": res["clocks"], "tuning": res["tuning"]}
     print(json.dumps(line))
     return 0
 

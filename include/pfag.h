@@ -74,6 +74,9 @@ int pfag_destroy(pfag_ctx *ctx);
  * phi, rho [Ntot][N][N], lum, ECM [N][N]; phin, rhon, hfunc_cell start at zero
  * and are then set to phi, rho (the copies at :92-98).  Synchronous. */
 int pfag_upload(pfag_ctx *ctx, const void *phi, const void *rho, const void *lum, const void *ecm);
+/* The same from device buffers of the current device (element type by the
+ * context's precision).  Synchronous. */
+int pfag_upload_device(pfag_ctx *ctx, const void *phi, const void *rho, const void *lum, const void *ecm);
 /* Device -> host state; any pointer may be NULL.  Synchronous. */
 int pfag_download(pfag_ctx *ctx, void *phi, void *rho, void *lum, void *ecm);
 
@@ -108,6 +111,57 @@ int pfag_get_velocity(pfag_ctx *ctx, void *vx, void *vy);
  * rimax + 2, the bound the reference's loops have).  A loop that reaches the
  * cap stops with PFAG_E_RELAX reported at the next synchronisation. */
 int pfag_set_relax_cap(pfag_ctx *ctx, int cap);
+
+/* Plain path only: on != 0 takes the cell areas (sum_s_kernels,
+ * useful_functions.cpp:179-184), sum_ecm (cell_phase_functions.cpp:380-386)
+ * and the reshaping loops' rdev sums (cell_phase_functions.cpp:556-561,
+ * :848-854) in the reference's serial host order, one thread per sum adding
+ * the terms i-major with the reference's expression, so each sum rounds as
+ * the host build's does on the same state.  Slow (a thread walks the grid);
+ * for parity studies.  The fused path returns PFAG_E_UNSUPPORTED. */
+int pfag_set_serial_sums(pfag_ctx *ctx, int on);
+
+/* A seeded synthetic organoid generated on the device instead of uploaded:
+ * phi_n = 0.5 (1 - tanh((r_n - radius)/2)) about centres[2n], centres[2n+1]
+ * (grid coordinates i, j; host array of Ntot pairs), rho_n = 1 where
+ * 0.05 < phi_n < 0.95 times (1 + 0.01 u) with u uniform in [-1, 1) from a
+ * hash of (seed, site), lumen 0, ECM 0.5 (1 + tanh((r - env_radius)/2))
+ * about the mean centre; then everything pfag_upload does after its copies.
+ * For workloads whose state is too large to build on the host.  Synchronous.
+ * No counterpart in the reference (it reads ini_*.bin files). */
+int pfag_seed_organoid(pfag_ctx *ctx, const double *centres, double radius, double env_radius,
+                       unsigned long long seed);
+
+/* Fused path: launch shapes of the step's persistent relaxation kernel and
+ * phi update (the knobs the batched sweep's autotuner sets).  coop_blocks > 0
+ * caps the persistent kernel's grid (0: the default, every co-resident block
+ * up to the loops' task count); update_warps > 0 is the warp budget the phi
+ * update sizes its row tasks for (0: the default, one full wave of the GPU).
+ * The next step recaptures its graph.  No counterpart in the reference (its
+ * OpenACC runtime picks the launch shapes). */
+int pfag_set_launch_shape(pfag_ctx *ctx, int coop_blocks, long update_warps);
+
+/* ---- Batches: several organoids (fused-path contexts on the current device)
+ * advanced together, the in-process form of the reference's parameter sweep
+ * (main_code/setup_simulation.py:206-312 writes one folder and one batch job
+ * per member).  After each member's first two steps (the first eager, the
+ * second captured as its step graph) a batch step is ONE graph launch whose
+ * child graphs are the members' step graphs, with no dependencies between
+ * members, so the GPU runs them side by side.  Member order is the caller's
+ * (group members of one box size together: the autotuner's buckets).
+ * pfag_batch_step is synchronous and refreshes every member's observables
+ * and statistics; pfag_batch_step_async enqueues only (the members' streams
+ * wait for it, so per-member calls stay ordered after it).  A member whose
+ * step graph changes (a new relaxation cap, launch shape, debug flag) makes
+ * the next batch step rebuild the parent graph. */
+typedef struct pfag_batch pfag_batch;
+int pfag_batch_create(pfag_ctx *const *ctxs, int n, pfag_batch **out);
+int pfag_batch_step(pfag_batch *b, int it0, int nsteps);
+int pfag_batch_step_async(pfag_batch *b, int it0, int nsteps);
+int pfag_batch_sync(pfag_batch *b);
+void *pfag_batch_stream(pfag_batch *b);       /* cudaStream_t the parent graph is launched on */
+long pfag_batch_launch_count(pfag_batch *b);  /* kernel launches of the last step call */
+int pfag_batch_destroy(pfag_batch *b);
 
 /* Per-kernel CUDA-event timing of the fused path on the context's stream.
  * pfag_profile_read synchronises and returns the number of kernels (<= cap):
@@ -199,6 +253,50 @@ int pfag_write_text_snapshot(const void *table, int precision, int N, const char
 /* saving_out_functions (useful_functions.cpp:66-99): device state -> host
  * snapshot slot; phi_out/rho_out get Ntot*N*N, lum_out/ecm_out N*N elements. */
 int pfag_fn_saving_out_functions(pfag_ctx *ctx, void *phi_out, void *rho_out, void *lum_out, void *ecm_out);
+
+/* ---- Learned coarse-grid corrector: convolution kernels on tcgen05 ----------
+ * No counterpart in the reference (its step has no learned part).  Tensors are
+ * device buffers.  An activation is BF16 [B][H+2][W+2][C] (channels last,
+ * with a one-site zero halo that is the convolution's zero padding; the
+ * caller zeroes a buffer once, the kernels keep its halo zero); weights are
+ * BF16 [Cout][9][Cin], tap t = (dy+1)*3 + (dx+1); biases and gradients FP32.
+ * All work is enqueued on `stream` (a cudaStream_t, NULL for the default
+ * stream).  `err` is a device word: bit 0 is set when a kernel's bounded
+ * wait for its tensor-core work runs out (its outputs are then invalid). */
+/* y = act(conv3x3(x, w) + bias), act = GELU when gelu_on; pre (optional)
+ * receives the pre-activation.  (cin, cout) in {(16,32), (32,32), (32,16),
+ * (16,16)}; W up to about 1500. */
+int pfag_conv3x3(const void *x, const void *w, const float *bias, void *y, void *pre, int B, int H, int W,
+                 int cin, int cout, int gelu_on, unsigned *err, void *stream);
+/* dw[co][t][ci] += sum over sites of dz[q][co] x[q + off_t][ci]; db[co] +=
+ * sum of dz[q][co] (accumulates: zero dw, db first). */
+int pfag_conv3x3_wgrad(const void *x, const void *dz, float *dw, float *db, int B, int H, int W, int cin,
+                       int cout, unsigned *err, void *stream);
+/* dz = dy * GELU'(pre) (gelu_on) or dy, zero on the halo. */
+int pfag_conv_act_bwd(const void *dy, const void *pre, void *dz, int B, int H, int W, int c, int gelu_on,
+                      void *stream);
+/* wt[ci][t][co] = w[co][8-t][ci]: the input gradient is pfag_conv3x3 of dz with wt. */
+int pfag_conv_flip(const void *w, void *wt, int cin, int cout, void *stream);
+/* One Adam step (bias-corrected, step t >= 1) on FP32 parameters p with
+ * gradient g and moments m, v; pb (optional) receives BF16 copies; mask
+ * (optional) multiplies each update. */
+int pfag_adam(float *p, const float *g, float *m, float *v, void *pb, const float *mask, int n, float lr,
+              float b1, float b2, float eps, int t, void *stream);
+/* Squared error of the first nout channels of out (C = 16 channels) against
+ * target [B][H][W][nout] (FP32): *loss += the sum, dout = 2 scale (out -
+ * target) on those channels and sites, zero elsewhere. */
+int pfag_conv_mse(const void *out, const float *target, void *dout, float *loss, int B, int H, int W, int c,
+                  int nout, float scale, void *stream);
+/* The corrector's input on every cell's FFT box (M = 2 zone_size - 2) of a
+ * context: x0 [Ntot][M+2][M+2][16] BF16 gets (s_phi phi, s_rho rho,
+ * s_v vx, s_v vy, 0...) of the last step (the velocity needs
+ * pfag_set_debug(ctx, 1) before that step; without it those channels are
+ * zero); enqueued on the context's stream. */
+int pfag_corrector_gather(pfag_ctx *ctx, void *x0, float s_phi, float s_rho, float s_v);
+/* phi += s_phi out[..0], rho += s_rho out[..1] on every cell's FFT box of a
+ * fused-path context, then the centroid sums the next step starts from are
+ * taken again from the corrected phi; enqueued on the context's stream. */
+int pfag_corrector_apply(pfag_ctx *ctx, const void *out, float s_phi, float s_rho);
 
 #ifdef __cplusplus
 }

@@ -55,7 +55,7 @@ _lib = None
 EXPORTS = [
     "pfag_last_error", "pfag_version", "pfag_create", "pfag_destroy", "pfag_upload", "pfag_download",
     "pfag_step", "pfag_step_async", "pfag_sync", "pfag_get_areas", "pfag_get_centres", "pfag_get_stats",
-    "pfag_get_cell_iters", "pfag_set_relax_cap", "pfag_set_debug", "pfag_get_velocity", "pfag_device_state", "pfag_stream", "pfag_launch_count",
+    "pfag_get_cell_iters", "pfag_set_relax_cap", "pfag_set_serial_sums", "pfag_set_debug", "pfag_get_velocity", "pfag_device_state", "pfag_stream", "pfag_launch_count",
     "pfag_fn_find_centres_cells", "pfag_fn_create_turnover_rates_tensions",
     "pfag_fn_compute_hfunc_3d_tables_kernels_loop_n", "pfag_fn_compute_all_hfunc_2d_tables_kernels",
     "pfag_fn_compute_normal_grad_phi", "pfag_fn_compute_prod_norm_delta", "pfag_fn_compute_psi_kernels",
@@ -63,6 +63,10 @@ EXPORTS = [
     "pfag_fn_reshaping_lumen_or_ECM", "pfag_fn_compute_normal_to_phi", "pfag_fn_update_all_cells",
     "pfag_fn_reshaping_cells", "pfag_fn_copy_back", "pfag_fn_saving_out_functions",
     "pfag_generate_initial", "pfag_observables_async", "pfag_snapshot_async", "pfag_snapshot_wait", "pfag_write_text_snapshot",
+    "pfag_seed_organoid", "pfag_set_launch_shape", "pfag_batch_create", "pfag_batch_step", "pfag_batch_step_async", "pfag_batch_sync",
+    "pfag_batch_stream", "pfag_batch_launch_count", "pfag_batch_destroy",
+    "pfag_upload_device", "pfag_conv3x3", "pfag_conv3x3_wgrad", "pfag_conv_act_bwd", "pfag_conv_flip", "pfag_adam",
+    "pfag_conv_mse", "pfag_corrector_gather", "pfag_corrector_apply",
 ]
 
 
@@ -88,6 +92,7 @@ def lib() -> ctypes.CDLL:
         L.pfag_set_debug.argtypes = [vp, ctypes.c_int]
         L.pfag_get_cell_iters.argtypes = [vp, vp]
         L.pfag_set_relax_cap.argtypes = [vp, ctypes.c_int]
+        L.pfag_set_serial_sums.argtypes = [vp, ctypes.c_int]
         L.pfag_get_velocity.argtypes = [vp, vp, vp]
         L.pfag_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
                                         ctypes.POINTER(vp)]
@@ -98,6 +103,27 @@ def lib() -> ctypes.CDLL:
         L.pfag_stream.restype = vp
         L.pfag_launch_count.argtypes = [vp]
         L.pfag_launch_count.restype = ctypes.c_long
+        L.pfag_set_launch_shape.argtypes = [vp, ctypes.c_int, ctypes.c_long]
+        L.pfag_seed_organoid.argtypes = [vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong]
+        L.pfag_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
+        L.pfag_batch_step.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.pfag_batch_step_async.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.pfag_batch_sync.argtypes = [vp]
+        L.pfag_batch_stream.argtypes = [vp]
+        L.pfag_batch_stream.restype = vp
+        L.pfag_batch_launch_count.argtypes = [vp]
+        L.pfag_batch_launch_count.restype = ctypes.c_long
+        L.pfag_batch_destroy.argtypes = [vp]
+        i, f = ctypes.c_int, ctypes.c_float
+        L.pfag_upload_device.argtypes = [vp, vp, vp, vp, vp]
+        L.pfag_conv3x3.argtypes = [vp, vp, vp, vp, vp, i, i, i, i, i, i, vp, vp]
+        L.pfag_conv3x3_wgrad.argtypes = [vp, vp, vp, vp, i, i, i, i, i, vp, vp]
+        L.pfag_conv_act_bwd.argtypes = [vp, vp, vp, i, i, i, i, i, vp]
+        L.pfag_conv_flip.argtypes = [vp, vp, i, i, vp]
+        L.pfag_adam.argtypes = [vp, vp, vp, vp, vp, vp, i, f, f, f, f, i, vp]
+        L.pfag_conv_mse.argtypes = [vp, vp, vp, vp, i, i, i, i, i, f, vp]
+        L.pfag_corrector_gather.argtypes = [vp, vp, f, f, f]
+        L.pfag_corrector_apply.argtypes = [vp, vp, f, f]
         L.pfag_generate_initial.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int]
         L.pfag_observables_async.argtypes = [vp, vp, vp, vp, vp]
         L.pfag_snapshot_async.argtypes = [vp, vp, vp, vp, vp]
@@ -220,6 +246,25 @@ class Simulation:
     def set_relax_cap(self, cap: int):
         check(lib().pfag_set_relax_cap(self.h, int(cap)))
 
+    def set_serial_sums(self, on: bool = True):
+        """Plain path: take the areas, sum_ecm and the relaxation checks' sums
+        in the reference's serial host order (one thread per cell)."""
+        check(lib().pfag_set_serial_sums(self.h, 1 if on else 0))
+
+    def upload_device(self, phi: int, rho: int, lum: int, ecm: int):
+        """State from device buffers (pointers) of the context's element type."""
+        check(lib().pfag_upload_device(self.h, *[ctypes.c_void_p(int(x)) for x in (phi, rho, lum, ecm)]))
+
+    def seed_organoid(self, centres, radius: float, env_radius: float, seed: int):
+        """Generate the seeded organoid on the device (pfag_seed_organoid)."""
+        c = np.ascontiguousarray(centres, dtype=np.float64).reshape(-1, 2)
+        if c.shape[0] != self.ncells:
+            raise ValueError(f"{c.shape[0]} centres for {self.ncells} cells")
+        check(lib().pfag_seed_organoid(self.h, _ptr(c), float(radius), float(env_radius), int(seed)))
+
+    def set_launch_shape(self, coop_blocks: int = 0, update_warps: int = 0):
+        check(lib().pfag_set_launch_shape(self.h, int(coop_blocks), int(update_warps)))
+
     def set_debug(self, flags: int = 1):
         check(lib().pfag_set_debug(self.h, int(flags)))
 
@@ -252,3 +297,41 @@ class Simulation:
         """Call one per-function entry point, e.g. fn("find_centres_cells")."""
         f = getattr(lib(), "pfag_fn_" + name)
         check(f(self.h, *args))
+
+
+class Batch:
+    """Fused-path simulations advanced together: one graph launch per step over
+    every member (pfag_batch_*).  The members stay owned by the caller."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)
+        arr = (ctypes.c_void_p * len(self.sims))(*[s.h for s in self.sims])
+        h = ctypes.c_void_p()
+        check(lib().pfag_batch_create(arr, len(self.sims), ctypes.byref(h)))
+        self.h = h
+
+    def step(self, it0: int, nsteps: int = 1):
+        check(lib().pfag_batch_step(self.h, int(it0), int(nsteps)))
+
+    def step_async(self, it0: int, nsteps: int = 1):
+        check(lib().pfag_batch_step_async(self.h, int(it0), int(nsteps)))
+
+    def sync(self):
+        check(lib().pfag_batch_sync(self.h))
+
+    def stream(self) -> int:
+        return lib().pfag_batch_stream(self.h) or 0
+
+    def launch_count(self) -> int:
+        return int(lib().pfag_batch_launch_count(self.h))
+
+    def close(self):
+        if self.h:
+            lib().pfag_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

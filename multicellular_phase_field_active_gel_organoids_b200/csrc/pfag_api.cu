@@ -190,7 +190,24 @@ extern "C" int pfag_upload(pfag_ctx *c, const void *phi, const void *rho, const 
     PFAG_CUDA_CHECK(cudaMemcpyAsync(c->rho, rho, c->nc * rs, cudaMemcpyHostToDevice, c->stream));
     PFAG_CUDA_CHECK(cudaMemcpyAsync(c->lum, lum, c->ng * rs, cudaMemcpyHostToDevice, c->stream));
     PFAG_CUDA_CHECK(cudaMemcpyAsync(c->ecm, ecm, c->ng * rs, cudaMemcpyHostToDevice, c->stream));
-    // run_with_active_gels.cpp:70-75 zero phin, rhon, hfunc_cell; :92-98 then copy
+    return pfag_after_upload(c);
+}
+
+extern "C" int pfag_upload_device(pfag_ctx *c, const void *phi, const void *rho, const void *lum, const void *ecm) {
+    if (!c || !phi || !rho || !lum || !ecm) { pfag_set_error("null argument"); return PFAG_E_ARG; }
+    const size_t rs = c->rsz;
+    PFAG_CUDA_CHECK(cudaMemcpyAsync(c->phi, phi, c->nc * rs, cudaMemcpyDeviceToDevice, c->stream));
+    PFAG_CUDA_CHECK(cudaMemcpyAsync(c->rho, rho, c->nc * rs, cudaMemcpyDeviceToDevice, c->stream));
+    PFAG_CUDA_CHECK(cudaMemcpyAsync(c->lum, lum, c->ng * rs, cudaMemcpyDeviceToDevice, c->stream));
+    PFAG_CUDA_CHECK(cudaMemcpyAsync(c->ecm, ecm, c->ng * rs, cudaMemcpyDeviceToDevice, c->stream));
+    return pfag_after_upload(c);
+}
+
+// The state phi, rho, lum, ECM is on the device: the rest of the set-up
+// main does before its loop (run_with_active_gels.cpp:70-75 zero phin, rhon,
+// hfunc_cell; :92-98 then copy), the fused path's upload checks; synchronous.
+int pfag_after_upload(pfag_ctx *c) {
+    const size_t rs = c->rsz;
     PFAG_CUDA_CHECK(cudaMemsetAsync(c->hfunc, 0, c->nc * rs, c->stream));
     PFAG_CUDA_CHECK(cudaMemcpyAsync(c->phin, c->phi, c->nc * rs, cudaMemcpyDeviceToDevice, c->stream));
     PFAG_CUDA_CHECK(cudaMemcpyAsync(c->rhon, c->rho, c->nc * rs, cudaMemcpyDeviceToDevice, c->stream));
@@ -279,6 +296,16 @@ extern "C" int pfag_get_stats(pfag_ctx *c, pfag_stats *st) {
 extern "C" int pfag_set_relax_cap(pfag_ctx *c, int cap) {
     if (!c || cap < 1) { pfag_set_error("relax cap must be >= 1"); return PFAG_E_ARG; }
     c->relax_cap = cap;
+    return PFAG_OK;
+}
+
+extern "C" int pfag_set_serial_sums(pfag_ctx *c, int on) {
+    if (!c) return PFAG_E_ARG;
+    if (on && c->path != PFAG_PATH_PLAIN) {
+        pfag_set_error("serial-order sums exist on the plain path only");
+        return PFAG_E_UNSUPPORTED;
+    }
+    c->serial_sums = on ? 1 : 0;
     return PFAG_OK;
 }
 

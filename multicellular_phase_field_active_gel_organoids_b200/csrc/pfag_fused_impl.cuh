@@ -28,6 +28,7 @@
 #include "pfag_internal.cuh"
 #include "pfag_fft.cuh"
 #include "pfag_regfft.cuh"
+#include "pfag_bluestein.cuh"
 #include <cooperative_groups.h>
 #include <algorithm>
 #include <climits>
@@ -86,12 +87,13 @@ struct FusedRes {
     bool fork;
     int npsi;
     int coop_r;             // co-resident block count of the persistent kernel
-    bool generic;           // box not a power of two in 16..1024: cuFFT-based spectral passes
-    cufftHandle gplan;      // their batched 2-D transform (Ntot boxes, in place)
-    cufftHandle gplan_xy;   // pi_xy's real 2-D transform
-    cufftHandle gplan_r2c, gplan_c2r;   // the fluxes' 1-D real row transforms
-    bool gplan_ok, gplan_xy_ok, gplan_r2c_ok, gplan_c2r_ok;
-    void *Gsp;              // the fluxes' half spectra [2][Ntot][M][M/2+1] complex
+    int coop_default;       // its value before any launch-shape setting
+    long upd_default;       // the phi update's warp budget before any launch-shape setting
+    bool generic;           // box not a power of two in 16..1024: Bluestein passes (M <= 512)
+    int blue_L;             // their inner power-of-two length (>= 2M-1, at least 32)
+    void *btw, *bcw, *bwf, *bhdi;   // their tables (pfag_bluestein.cuh), in the context's precision
+    double *bh;             // the derivative kernel h in FP64 (table scratch)
+    void *Gsp;              // pi_xy's half spectrum [Ntot][M][M/2+1] complex
     long upd_warps;         // co-resident warps of kf_update_rows (FP32)
     size_t upd_smem;        // its row ring
     int logm, rows_blk, grp_cols;
@@ -1232,13 +1234,13 @@ __global__ void __launch_bounds__(BT, 1280 / BT) kr_boxB(typename Cplx<real>::ty
     store_cols_fixed<cx, M, NSP, BT>(Y1 + (size_t)n * M * M, Z1, cs);
 }
 
-// ---- spectral solve for any box size (M not a power of two, e.g. the
-//      reference's default zone_size 200, M = 398): the same steps as the
-//      register passes with cuFFT's batched transforms (three 2-D ones and a
-//      1-D real pair per cell instead of the reference's ten 2-D ones;
-//      update_all_cortices, rho_functions.cpp:409-471).  Y1, Y2: [Ntot][M][M]
-//      complex (Y2 also as two real [Ntot][M][M] planes for the fluxes); Rb:
-//      R; cm: the class map [Ntot][M][M] (row-major, not transposed).
+// ---- spectral solve for any even box size up to 512 that is not a power of
+//      two (the reference's default zone_size 200, M = 398): the same steps as
+//      the register passes with the Bluestein transforms of pfag_bluestein.cuh
+//      (update_all_cortices, rho_functions.cpp:409-471).  Y1, Y2: [Ntot][M][M]
+//      complex (Y2 also as two real [Ntot][M][M] planes: pi_xy, then the
+//      fluxes); Rb: R; cm: the class map [Ntot][M][M] (row-major, not
+//      transposed).
 
 // stresses, reaction and class on the box: Y1 = pi_xx + i pi_yy, Y2 (as reals) = pi_xy
 template <typename real>
@@ -1316,89 +1318,6 @@ __global__ void kg_velocity(typename Cplx<real>::type *__restrict__ Y1, const ty
     pb.x = hx.x + hy.y; pb.y = hy.x - hx.y;
     y1[e] = pa;
     if (eb != e) y1[eb] = pb;
-}
-
-// fluxes (load_fft_rho_v, rho_functions.cpp:267-284): Y1 holds M^2 (vx + i vy).
-// The divergence of update_fft_rho is separable (the transforms along the
-// other axis cancel): Re(IFFT2(-i ir FFT2(Fx)))/M^2 = Re(IFFT_i(-i ir FFT_i(Fx)))/M
-// along columns, likewise Fy along rows, so the fluxes go to real rows for
-// 1-D real transforms: Fr[0][n] = Fx transposed (its columns as rows),
-// Fr[1][n] = Fy.  32 x 32 tiles through shared memory keep both coalesced.
-template <typename real>
-__global__ void __launch_bounds__(256) kg_flux(const typename Cplx<real>::type *__restrict__ Y1,
-                                               real *__restrict__ Fr, const real *__restrict__ rho,
-                                               const int *__restrict__ xc, const int *__restrict__ yc, BoxArgs a,
-                                               real *__restrict__ vdx, real *__restrict__ vdy) {
-    __shared__ real tile[32][33];
-    const int n = blockIdx.z, M = a.M, N = a.N;
-    const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
-    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
-    const real mm = (real)((double)M * (double)M);
-    const size_t cell = (size_t)n * M * M;
-    real *fxT = Fr + cell, *fy = Fr + (size_t)a.Ntot * M * M + cell;
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-        const int i = i0 + r, j = j0 + threadIdx.x;
-        if (i < M && j < M) {
-            const size_t o = (size_t)i * M + j;
-            const typename Cplx<real>::type v = Y1[cell + o];
-            const real rr = rho[(size_t)n * N * N + (size_t)(bi + i) * N + bj + j];
-            tile[r][threadIdx.x] = rr * v.x / mm;
-            fy[o] = rr * v.y / mm;
-            if (vdx) { vdx[cell + o] = v.x / mm; vdy[cell + o] = v.y / mm; }
-        }
-    }
-    __syncthreads();
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-        const int j = j0 + r, i = i0 + threadIdx.x;
-        if (i < M && j < M) fxT[(size_t)j * M + i] = tile[threadIdx.x][r];
-    }
-}
-
-// the half spectra of the flux rows times -i k (k the row wavenumber index,
-// 0 at the Nyquist bin: the Re() of update_fft_rho's odd multiplier)
-template <typename real>
-__global__ void kg_dmul(typename Cplx<real>::type *__restrict__ S, long rows, int M) {
-    const int H = M / 2 + 1;
-    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= rows * H) return;
-    const int k = (int)(e % H);
-    const real kk = (real)((k == M / 2) ? 0 : k);
-    const typename Cplx<real>::type z = S[e];
-    typename Cplx<real>::type y;
-    y.x = kk * z.y;
-    y.y = -kk * z.x;
-    S[e] = y;
-}
-
-// rho <- rho + dt R + dt kfac (dFx + dFy) / M on the box (copy_to_rhon,
-// rho_functions.cpp:253-265, by linearity of the reference's spectral
-// update); Fr holds M times the two derivatives, the x one transposed
-template <typename real>
-__global__ void __launch_bounds__(256) kg_rho(const real *__restrict__ Fr, const real *__restrict__ Rb,
-                                              real *__restrict__ rho, const int *__restrict__ xc,
-                                              const int *__restrict__ yc, BoxArgs a) {
-    __shared__ real tile[32][33];
-    const int n = blockIdx.z, M = a.M, N = a.N;
-    const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
-    const size_t cell = (size_t)n * M * M;
-    const real *dxT = Fr + cell, *dy = Fr + (size_t)a.Ntot * M * M + cell;
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {            // dxT rows j0.., columns i0..
-        const int j = j0 + r, i = i0 + threadIdx.x;
-        if (i < M && j < M) tile[r][threadIdx.x] = dxT[(size_t)j * M + i];
-    }
-    __syncthreads();
-    const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
-    const real dtk = (real)(a.dt * a.kfac), inv_m = (real)(1.0 / (double)M), dt = (real)a.dt;
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-        const int i = i0 + r, j = j0 + threadIdx.x;
-        if (i < M && j < M) {
-            const size_t o = (size_t)i * M + j;
-            real &ro = rho[(size_t)n * N * N + (size_t)(bi + i) * N + bj + j];
-            const real ti = dtk * (tile[threadIdx.x][r] * inv_m);
-            const real yy = dtk * (dy[o] * inv_m);
-            ro = ro + dt * Rb[cell + o] + (ti + yy);
-        }
-    }
 }
 
 // ---- phi update (cell_phase_functions.cpp:126-217) + normals
@@ -2395,9 +2314,19 @@ struct Fused {
         int logm = 0;
         while ((1 << logm) < M) logm++;
         // power-of-two boxes from 16 to 1024: the hand-written FFT passes; any
-        // other box: the cuFFT-based generic passes (kg_*)
+        // other box up to 512: the Bluestein passes (kg_*, kbl_*)
         r->generic = (1 << logm) != M || M < 16 || M > 1024;
         if (M < 2) { pfag_set_error("zone_size %d gives no FFT box", c->zone); return PFAG_E_UNSUPPORTED; }
+        if (r->generic) {
+            if (M > 512 || (M & 1)) {
+                pfag_set_error("fused path: FFT box %d (zone_size %d) is neither a power of two in 16..1024 nor an "
+                               "even size up to 512; the plain path supports it", M, c->zone);
+                return PFAG_E_UNSUPPORTED;
+            }
+            int L = 32;
+            while (L < 2 * M - 1) L <<= 1;
+            r->blue_L = L;
+        }
         if (c->Ntot > 1024) { pfag_set_error("fused path supports at most 1024 cells"); return PFAG_E_UNSUPPORTED; }
         r->logm = logm;
         const size_t cs = sizeof(cx);
@@ -2455,6 +2384,8 @@ struct Fused {
                                                                            r->upd_smem));
             r->upd_warps = (long)nsm * std::max(per, 1) * (UPD_THREADS / 32);
         }
+        r->coop_default = r->coop_r;
+        r->upd_default = r->upd_warps;
         return PFAG_OK;
     }
 
@@ -2466,27 +2397,20 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaMalloc(&r->Rb, (size_t)c->Ntot * mm * rs));
         PFAG_CUDA_CHECK(cudaMalloc(&r->clsT, (size_t)c->Ntot * mm));
         if (r->generic) {
-            int dims[2] = {c->M, c->M};
-            cufftResult e = cufftPlanMany(&r->gplan, 2, dims, nullptr, 1, (int)mm, nullptr, 1, (int)mm,
-                                          sizeof(real) == 8 ? CUFFT_Z2Z : CUFFT_C2C, c->Ntot);
-            if (e != CUFFT_SUCCESS) { pfag_set_error("cufftPlanMany (%d x %d, batch %d): error %d", c->M, c->M, c->Ntot, (int)e); return PFAG_E_CUDA; }
-            r->gplan_ok = true;
-            // pi_xy: Ntot real 2-D transforms (half spectra into Gsp)
-            int hdims[2] = {c->M, c->M / 2 + 1};
-            e = cufftPlanMany(&r->gplan_xy, 2, dims, dims, 1, (int)mm, hdims, 1, c->M * (c->M / 2 + 1),
-                              sizeof(real) == 8 ? CUFFT_D2Z : CUFFT_R2C, c->Ntot);
-            if (e != CUFFT_SUCCESS) { pfag_set_error("cufftPlanMany (R2C %d x %d, batch %d): error %d", c->M, c->M, c->Ntot, (int)e); return PFAG_E_CUDA; }
-            r->gplan_xy_ok = true;
-            // the fluxes' rows: 2 Ntot M real transforms of length M and their inverses
-            int m1 = c->M, h1 = c->M / 2 + 1;
-            const int rows = 2 * c->Ntot * c->M;
-            e = cufftPlanMany(&r->gplan_r2c, 1, &m1, &m1, 1, m1, &h1, 1, h1, sizeof(real) == 8 ? CUFFT_D2Z : CUFFT_R2C, rows);
-            if (e != CUFFT_SUCCESS) { pfag_set_error("cufftPlanMany (R2C %d, batch %d): error %d", m1, rows, (int)e); return PFAG_E_CUDA; }
-            r->gplan_r2c_ok = true;
-            e = cufftPlanMany(&r->gplan_c2r, 1, &m1, &h1, 1, h1, &m1, 1, m1, sizeof(real) == 8 ? CUFFT_Z2D : CUFFT_C2R, rows);
-            if (e != CUFFT_SUCCESS) { pfag_set_error("cufftPlanMany (C2R %d, batch %d): error %d", m1, rows, (int)e); return PFAG_E_CUDA; }
-            r->gplan_c2r_ok = true;
-            PFAG_CUDA_CHECK(cudaMalloc(&r->Gsp, (size_t)rows * h1 * 2 * rs));
+            const int M = c->M, L = r->blue_L;
+            PFAG_CUDA_CHECK(cudaMalloc(&r->Gsp, (size_t)c->Ntot * M * (M / 2 + 1) * 2 * rs));
+            PFAG_CUDA_CHECK(cudaMalloc(&r->btw, (size_t)L * 2 * rs));
+            PFAG_CUDA_CHECK(cudaMalloc(&r->bcw, (size_t)M * 2 * rs));
+            PFAG_CUDA_CHECK(cudaMalloc(&r->bwf, (size_t)L * 2 * rs));
+            PFAG_CUDA_CHECK(cudaMalloc(&r->bhdi, (size_t)L * rs));
+            PFAG_CUDA_CHECK(cudaMalloc(&r->bh, (size_t)M * sizeof(double)));
+            const double dtk = c->dp.dt * c->dp.kfac;
+            kbl_tables1<cx><<<(std::max(L, M) + 127) / 128, 128, 0, c->stream>>>(M, L, dtk, (cx *)r->btw,
+                                                                                  (cx *)r->bcw, r->bh);
+            PFAG_CUDA_CHECK(cudaGetLastError());
+            kbl_tables2<cx><<<(L + 127) / 128, 128, 0, c->stream>>>(M, L, r->bh, (cx *)r->bwf, R(r->bhdi));
+            PFAG_CUDA_CHECK(cudaGetLastError());
+            PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
         }
         PFAG_CUDA_CHECK(cudaMalloc(&r->Jc, (size_t)c->Ntot * 2 * W * W * rs));
         PFAG_CUDA_CHECK(cudaMalloc(&r->Jl, 4 * c->ng * rs));
@@ -2553,7 +2477,7 @@ struct Fused {
         cudaStream_t s = c->stream;
         if (r->fork) PFAG_CUDA_CHECK(cudaStreamWaitEvent(s, r->ev_area, 0));
         const int z = c->zone, W = 2 * z + 2;
-        pfag_prof_begin(c, "kf_update");
+        pfag_prof_begin(c, sizeof(real) == 4 ? "kf_update_rows" : "kf_update_tiled");
         if constexpr (sizeof(real) == 4) {
             // row chunks: as many warp tasks as fit on the GPU at once (one wave), with at
             // least 16 rows per task (a task loads 8 rows beyond the ones it updates)
@@ -2742,24 +2666,36 @@ struct Fused {
     // primaries per block of the column passes (shared tile near 64 KB)
     static constexpr int GB = 4;
 
-    int fft(cx *buf, int dir) {
-        cufftResult e;
-        if constexpr (sizeof(real) == 8)
-            e = cufftExecZ2Z(r->gplan, (cufftDoubleComplex *)buf, (cufftDoubleComplex *)buf, dir);
-        else
-            e = cufftExecC2C(r->gplan, (cufftComplex *)buf, (cufftComplex *)buf, dir);
-        if (e != CUFFT_SUCCESS) { pfag_set_error("cufftExec: error %d", (int)e); return PFAG_E_CUDA; }
-        return PFAG_OK;
+    BlueTabs<cx> blue_tabs() {
+        BlueTabs<cx> tb;
+        tb.tw = (const cx *)r->btw; tb.cw = (const cx *)r->bcw; tb.wf = (const cx *)r->bwf;
+        tb.hdi = (const real *)r->bhdi;
+        return tb;
     }
 
-    // spectral solve on boxes of any size: stresses, 2-D transforms of the
-    // two stress spectra, k-space velocity, inverse, fluxes, transform, the
-    // divergence multiplier, inverse, new rho on the box (the phi update runs
-    // after the stress kernel, which has read rho, lum and ECM)
-    int box_generic(const BoxArgs &ba) {
+    // spectral solve on boxes of any even size up to 512 with Bluestein
+    // transforms of inner length L: stresses; forward row transforms (pi_xx +
+    // i pi_yy in place, pi_xy's rows in pairs to half spectra); forward column
+    // transforms; the k-space velocity; inverse column transforms; inverse
+    // row transforms with the fluxes and the row derivative; the column
+    // derivative and the new rho on the box.  The phi update runs after the
+    // stress kernel, which has read rho, lum and ECM.
+    template <int L>
+    int box_blue(const BoxArgs &ba) {
+        typedef BlueGeom<real, L> BGm;
         cudaStream_t s = c->stream;
-        const int M = c->M, Nt = c->Ntot;
-        cx *Y1 = (cx *)r->Y1, *Y2 = (cx *)r->Y2;
+        const int M = c->M, Nt = c->Ntot, N = c->N, z = c->zone, H = M / 2 + 1;
+        cx *Y1 = (cx *)r->Y1, *Y2 = (cx *)r->Y2, *Hs = (cx *)r->Gsp;
+        const BlueTabs<cx> tb = blue_tabs();
+        const size_t cs = sizeof(cx);
+        const size_t sm_rows = (size_t)(1 + BGm::GPB) * L * cs;
+        const size_t sm_cols = ((size_t)L + (size_t)BGm::GPB * (L + 1)) * cs;
+        PFAG_TRY(smem_at_least((const void *)kbl_rowsA<real, L>, sm_rows));
+        const size_t sm_rowsD = sm_rows + (size_t)BGm::GPB * 2 * M * sizeof(real);
+        PFAG_TRY(smem_at_least((const void *)kbl_rowsD<real, L>, sm_rowsD));
+        PFAG_TRY(smem_at_least((const void *)kbl_cols<real, L, false>, sm_cols));
+        PFAG_TRY(smem_at_least((const void *)kbl_cols<real, L, true>, sm_cols));
+        PFAG_TRY(smem_at_least((const void *)kbl_colsE<real, L>, sm_cols));
         const dim3 g((M * M + 255) / 256, Nt);
         pfag_prof_begin(c, "kg_stress");
         kg_stress<real><<<g, 256, 0, s>>>(R(c->phi), R(c->rho), R(c->lum), R(c->ecm), c->d_xc, c->d_yc, ba, Y1, Y2,
@@ -2767,46 +2703,58 @@ struct Fused {
         PFAG_LAUNCHED(c);
         if (r->fork) PFAG_CUDA_CHECK(cudaEventRecord(r->ev_boxA, s));
         PFAG_TRY(launch_update());
-        if (cufftSetStream(r->gplan, s) != CUFFT_SUCCESS) { pfag_set_error("cufftSetStream failed"); return PFAG_E_CUDA; }
-        // profiled segments: the transforms count with the kernel between them
-        pfag_prof_begin(c, "kg_spectra");
-        PFAG_TRY(fft(Y1, CUFFT_FORWARD));
         {
-            if (cufftSetStream(r->gplan_xy, s) != CUFFT_SUCCESS) { pfag_set_error("cufftSetStream failed"); return PFAG_E_CUDA; }
-            cufftResult e;
-            if constexpr (sizeof(real) == 8) e = cufftExecD2Z(r->gplan_xy, (double *)Y2, (cufftDoubleComplex *)r->Gsp);
-            else e = cufftExecR2C(r->gplan_xy, (float *)Y2, (cufftComplex *)r->Gsp);
-            if (e != CUFFT_SUCCESS) { pfag_set_error("cufftExec (R2C 2-D): error %d", (int)e); return PFAG_E_CUDA; }
+            const long tasks = (long)Nt * (M + M / 2);
+            pfag_prof_begin(c, "kbl_rowsA");
+            kbl_rowsA<real, L><<<(unsigned)((tasks + BGm::GPB - 1) / BGm::GPB), BGm::THREADS, sm_rows, s>>>(
+                Y1, (const real *)Y2, Hs, M, Nt, tb);
+            PFAG_LAUNCHED(c);
         }
-        kg_velocity<real><<<g, 256, 0, s>>>(Y1, (const cx *)r->Gsp, r->clsT, ba);
-        c->launches++;
-        PFAG_TRY(fft(Y1, CUFFT_INVERSE));
-        pfag_prof_end(c);
-        real *Fr = (real *)r->Y2;              // pass B is done with Y2: the fluxes' real rows
-        const dim3 gt((M + 31) / 32, (M + 31) / 32, Nt), bt(32, 8);
-        pfag_prof_begin(c, "kg_flux");
-        kg_flux<real><<<gt, bt, 0, s>>>(Y1, Fr, R(c->rho), c->d_xc, c->d_yc, ba, c->debug ? R(c->d_vx) : nullptr,
-                                        c->debug ? R(c->d_vy) : nullptr);
+        ColSet<cx> y1s{Y1, (long)M * M, M, M, (M + BGm::GPB - 1) / BGm::GPB};
+        ColSet<cx> hss{Hs, (long)M * H, H, H, (H + BGm::GPB - 1) / BGm::GPB};
+        ColSet<cx> none{Y1, 0, M, 0, 0};
+        pfag_prof_begin(c, "kbl_colsB");
+        kbl_cols<real, L, false><<<(unsigned)((long)Nt * (y1s.nblk + hss.nblk)), BGm::THREADS, sm_cols, s>>>(
+            y1s, hss, M, Nt, tb);
         PFAG_LAUNCHED(c);
-        pfag_prof_begin(c, "kg_div");
-        const long rows = 2L * Nt * M;
-        if (cufftSetStream(r->gplan_r2c, s) != CUFFT_SUCCESS || cufftSetStream(r->gplan_c2r, s) != CUFFT_SUCCESS) {
-            pfag_set_error("cufftSetStream failed");
-            return PFAG_E_CUDA;
+        pfag_prof_begin(c, "kg_velocity");
+        kg_velocity<real><<<g, 256, 0, s>>>(Y1, (const cx *)Hs, r->clsT, ba);
+        PFAG_LAUNCHED(c);
+        pfag_prof_begin(c, "kbl_colsC");
+        kbl_cols<real, L, true><<<(unsigned)((long)Nt * y1s.nblk), BGm::THREADS, sm_cols, s>>>(y1s, none, M, Nt,
+                                                                                                tb);
+        PFAG_LAUNCHED(c);
+        real *X = (real *)r->Y2;              // free once the row pass has read pi_xy: Fx, then the row term
+        {
+            const long tasks = (long)Nt * (M / 2);
+            pfag_prof_begin(c, "kbl_rowsD");
+            kbl_rowsD<real, L><<<(unsigned)((tasks + BGm::GPB - 1) / BGm::GPB), BGm::THREADS, sm_rowsD, s>>>(
+                Y1, X, R(c->rho), c->d_xc, c->d_yc, N, z, M, Nt, tb, c->debug ? R(c->d_vx) : nullptr,
+                c->debug ? R(c->d_vy) : nullptr);
+            PFAG_LAUNCHED(c);
         }
-        cufftResult e;
-        if constexpr (sizeof(real) == 8) e = cufftExecD2Z(r->gplan_r2c, (double *)Fr, (cufftDoubleComplex *)r->Gsp);
-        else e = cufftExecR2C(r->gplan_r2c, (float *)Fr, (cufftComplex *)r->Gsp);
-        if (e != CUFFT_SUCCESS) { pfag_set_error("cufftExec (R2C): error %d", (int)e); return PFAG_E_CUDA; }
-        const long nb = rows * (M / 2 + 1);
-        kg_dmul<real><<<(unsigned)((nb + 255) / 256), 256, 0, s>>>((cx *)r->Gsp, rows, M);
-        c->launches++;
-        if constexpr (sizeof(real) == 8) e = cufftExecZ2D(r->gplan_c2r, (cufftDoubleComplex *)r->Gsp, (double *)Fr);
-        else e = cufftExecC2R(r->gplan_c2r, (cufftComplex *)r->Gsp, (float *)Fr);
-        if (e != CUFFT_SUCCESS) { pfag_set_error("cufftExec (C2R): error %d", (int)e); return PFAG_E_CUDA; }
-        kg_rho<real><<<gt, bt, 0, s>>>(Fr, R(r->Rb), R(c->rho), c->d_xc, c->d_yc, ba);
-        PFAG_LAUNCHED(c);
+        {
+            const long tasks = (long)Nt * ((M / 2 + BGm::GPB - 1) / BGm::GPB);
+            pfag_prof_begin(c, "kbl_colsE");
+            kbl_colsE<real, L><<<(unsigned)tasks, BGm::THREADS, sm_cols, s>>>(X, R(c->rho), R(r->Rb), c->d_xc,
+                                                                              c->d_yc, N, z, M, Nt, c->dp.dt, tb);
+            PFAG_LAUNCHED(c);
+        }
         return PFAG_OK;
+    }
+
+    int box_generic(const BoxArgs &ba) {
+        switch (r->blue_L) {
+        case 32: return box_blue<32>(ba);
+        case 64: return box_blue<64>(ba);
+        case 128: return box_blue<128>(ba);
+        case 256: return box_blue<256>(ba);
+        case 512: return box_blue<512>(ba);
+        case 1024: return box_blue<1024>(ba);
+        default:
+            pfag_set_error("no Bluestein pass for inner length %d", r->blue_L);
+            return PFAG_E_UNSUPPORTED;
+        }
     }
 
     template <int MM>
@@ -2830,24 +2778,33 @@ struct Fused {
         PFAG_TRY(smem_at_least((const void *)kr_boxD2<real, MM>, smD2));
         cx *Y1 = (cx *)r->Y1, *Y2 = (cx *)r->Y2;
         const dim3 grow(MM / BG::ROWS, Nt);
-        pfag_prof_begin(c, "kf_boxA");
+        pfag_prof_begin(c, "kr_boxA");
         kr_boxA<real, MM><<<grow, BG::THREADS, smA, s>>>(R(c->phi), R(c->rho), R(c->lum), R(c->ecm), c->d_xc, c->d_yc,
                                                           ba, Y1, Y2, R(r->Rb), r->clsT);
         PFAG_LAUNCHED(c);
         if (r->fork) PFAG_CUDA_CHECK(cudaEventRecord(r->ev_boxA, s));
         PFAG_TRY(launch_update());
-        pfag_prof_begin(c, "kf_boxB");
+        pfag_prof_begin(c, "kr_boxB");
         kr_boxB<real, MM, GB, 256><<<dim3((MM / 2 + 1 + GB - 1) / GB, Nt), 256, smB, s>>>(Y1, Y2, r->clsT, ba);
         PFAG_LAUNCHED(c);
         real *X = (real *)r->Y2;          // pass B is done with Y2: Fx, then the row term
-        pfag_prof_begin(c, "kf_boxC");
+        pfag_prof_begin(c, "kr_boxC2");
         kr_boxC2<real, MM><<<grow, BG::THREADS, smC, s>>>(Y1, X, R(c->rho), c->d_xc, c->d_yc, ba,
                                                            c->debug ? R(c->d_vx) : nullptr,
                                                            c->debug ? R(c->d_vy) : nullptr);
         PFAG_LAUNCHED(c);
-        pfag_prof_begin(c, "kf_boxD");
+        pfag_prof_begin(c, "kr_boxD2");
         kr_boxD2<real, MM><<<dim3(MM / BD::COLS, Nt), 256, smD2, s>>>(X, R(c->rho), R(r->Rb), c->d_xc, c->d_yc, ba);
         PFAG_LAUNCHED(c);
+        return PFAG_OK;
+    }
+
+    // centroid sums over every support rectangle from the current phi (after
+    // phi was changed between steps), for the next step's centroids
+    int recentre() {
+        PFAG_CUDA_CHECK(cudaMemsetAsync(c->d_cacc, 0, sizeof(long long) * 3 * c->Ntot, c->stream));
+        kf_centroid<real><<<dim3(64, c->Ntot), FT, 0, c->stream>>>(R(c->phi), r->rect, c->N, c->d_cacc);
+        PFAG_CUDA_CHECK(cudaGetLastError());
         return PFAG_OK;
     }
 
@@ -2878,6 +2835,8 @@ struct Fused {
 
 // Entry points instantiated once per precision (pfag_fused_f64.cu, pfag_fused_f32.cu).
 template <typename real> int fused_alloc_t(pfag_ctx *c) { return Fused<real>(c).alloc(); }
+template <typename real> int fused_stats_t(pfag_ctx *c) { return Fused<real>(c).stats(); }
+template <typename real> int fused_recentre_t(pfag_ctx *c) { return Fused<real>(c).recentre(); }
 template <typename real> int fused_upload_t(pfag_ctx *c) { return Fused<real>(c).upload_hook(); }
 inline void fused_drop_graph(FusedRes *r) {
     if (r->graph_ok) { cudaGraphExecDestroy(r->gexec); cudaGraphDestroy(r->graph); }
@@ -2893,7 +2852,7 @@ template <typename real> int fused_step_t(pfag_ctx *c, bool sync_host) {
     FusedRes *r = F(c);
     const bool graphable = !pfag_prof_on(c) && !c->debug && !std::getenv("PFAG_NO_GRAPH");
     const long key = (long)c->relax_cap;
-    if (r->graph_ok && (!graphable || r->graph_key != key)) {
+    if (r->graph_ok && r->graph_key != key) {
         fused_drop_graph(r);
         r->graph_state = 0;
     }
@@ -2919,7 +2878,7 @@ template <typename real> int fused_step_t(pfag_ctx *c, bool sync_host) {
         (void)cudaGetLastError();   // a refused capture leaves a non-sticky error
     }
     int rc = PFAG_OK;
-    if (r->graph_ok && !r->ring_pending) {
+    if (r->graph_ok && !r->ring_pending && graphable) {
         PFAG_CUDA_CHECK(cudaGraphLaunch(r->gexec, c->stream));
         c->launches += r->graph_launches;
     } else {

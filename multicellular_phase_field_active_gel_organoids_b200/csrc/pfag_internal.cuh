@@ -107,6 +107,7 @@ struct pfag_ctx {
     long launches;
     int debug;
     int relax_cap;        // device-side loop bound (fused path)
+    int serial_sums;      // plain path: reductions in the reference's serial host order
     void *d_vx, *d_vy;
     // fused-path resources (opaque, owned by pfag_fused.cu)
     void *fused;
@@ -132,6 +133,8 @@ void pfag_fused_free(pfag_ctx *ctx);
 int pfag_fused_upload_hook(pfag_ctx *ctx);
 int pfag_fused_step(pfag_ctx *ctx, int it, bool sync_host);
 int pfag_check_device_error(pfag_ctx *ctx);
+int pfag_after_upload(pfag_ctx *ctx);
+int pfag_fused_recentre(pfag_ctx *ctx);
 
 // ---------------------------------------------------------------------------
 // Device helpers shared by both paths.

@@ -223,6 +223,56 @@ __global__ void k_sum_s_finalize(const double *__restrict__ part, int nblk, int 
     f0[n] = alpha * (s0 - a);
 }
 
+// Serial-order sums (pfag_set_serial_sums): one thread per cell adds the terms
+// in the order and with the expression of the reference's host loops, i-major
+// with j inner.  sum_s_kernels (useful_functions.cpp:179-184):
+// sum += h*dx*dx over the full grid; the reshaping check
+// (cell_phase_functions.cpp:556-561): rdev += |phin-phi|*dx*dx/N_current over
+// the zone; update_lumen_and_ECM's sum_ecm (:380-386) and the lumen/ECM check
+// (:848-854): sum += v*dx*dx over the full grid.  Compiled without
+// contraction, each partial sum then rounds as the host build's does.
+template <typename real>
+__global__ void k_serial_sum_cells(const real *__restrict__ h, int N, int ncells, double dx,
+                                   double *__restrict__ out) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ncells) return;
+    const real *p = h + (size_t)n * N * N;
+    double acc = 0.0;
+    for (int i = 0; i < N; i++)
+        for (int j = 0; j < N; j++) acc += (double)p[(size_t)i * N + j] * dx * dx;
+    out[n] = acc;
+}
+
+template <typename real>
+__global__ void k_serial_absdiff(const real *__restrict__ a, const real *__restrict__ b, int N, double dx,
+                                 double *__restrict__ out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double acc = 0.0;
+    for (int i = 0; i < N; i++)
+        for (int j = 0; j < N; j++) {
+            const size_t o = (size_t)i * N + j;
+            acc += fabs((double)a[o] - (double)b[o]) * dx * dx;
+        }
+    *out = acc;
+}
+
+template <typename real>
+__global__ void k_serial_cell_rdev(const real *__restrict__ pn, const real *__restrict__ p,
+                                   const int *__restrict__ xc, const int *__restrict__ yc, int N, int z, int ncells,
+                                   double dx, double ncur, const int *__restrict__ active,
+                                   double *__restrict__ out) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ncells) return;
+    double acc = 0.0;
+    if (active[n])
+        for (int i = xc[n] - z; i < xc[n] + z; i++)
+            for (int j = yc[n] - z; j < yc[n] + z; j++) {
+                const size_t o = cidx(n, i, j, N);
+                acc += fabs((double)pn[o] - (double)p[o]) * dx * dx / ncur;
+            }
+    out[n] = acc;
+}
+
 // ---- update_all_cortices helpers (rho_functions.cpp:32-284, useful_functions.cpp:605-625)
 template <typename real>
 __global__ void k_pi(const real *__restrict__ rho, const real *__restrict__ g, const real *__restrict__ phi,
@@ -744,10 +794,17 @@ struct Plain {
         return PFAG_OK;
     }
     int sum_s() {
-        k_sum_cells<real><<<dim3(RED_BLOCKS, c->Ntot), RED_THREADS, 0, c->stream>>>(R(c->hfunc), c->ng,
-                                                                                   c->dp.dx * c->dp.dx, c->d_part);
+        int nblk = RED_BLOCKS;
+        if (c->serial_sums) {
+            nblk = 1;
+            k_serial_sum_cells<real><<<(c->Ntot + 63) / 64, 64, 0, c->stream>>>(R(c->hfunc), c->N, c->Ntot,
+                                                                                c->dp.dx, c->d_part);
+        } else {
+            k_sum_cells<real><<<dim3(RED_BLOCKS, c->Ntot), RED_THREADS, 0, c->stream>>>(R(c->hfunc), c->ng,
+                                                                                       c->dp.dx * c->dp.dx, c->d_part);
+        }
         PFAG_LAUNCHED(c);
-        k_sum_s_finalize<<<(c->Ntot + 127) / 128, 128, 0, c->stream>>>(c->d_part, RED_BLOCKS, c->Ntot, c->dp.alpha,
+        k_sum_s_finalize<<<(c->Ntot + 127) / 128, 128, 0, c->stream>>>(c->d_part, nblk, c->Ntot, c->dp.alpha,
                                                                          c->dp.s0, c->d_s, c->d_f0);
         PFAG_LAUNCHED(c);
         return PFAG_OK;
@@ -799,6 +856,11 @@ struct Plain {
         return bc_cells(c->rhon, c->Ntot);
     }
     int sum_reduce_2d(const void *a, const void *b, double scale, double *out) {
+        if (c->serial_sums) {
+            k_serial_absdiff<real><<<1, 32, 0, c->stream>>>(R((void *)a), R((void *)b), c->N, c->dp.dx, out);
+            PFAG_LAUNCHED(c);
+            return PFAG_OK;
+        }
         k_absdiff_sum<real><<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(R((void *)a), R((void *)b), c->ng, scale,
                                                                       c->d_part);
         PFAG_LAUNCHED(c);
@@ -809,11 +871,16 @@ struct Plain {
     int lum_ecm_update() {
         const int N = c->N;
         // sum_ecm = sum h(ECM) dx^2 over the full grid (FP64)
-        k_sum_cells<real><<<dim3(RED_BLOCKS, 1), RED_THREADS, 0, c->stream>>>(R(c->hecm), c->ng, c->dp.dx * c->dp.dx,
-                                                                             c->d_part);
-        PFAG_LAUNCHED(c);
-        k_sum_partials<<<1, 32, 0, c->stream>>>(c->d_part, RED_BLOCKS, c->d_scal + 0);
-        PFAG_LAUNCHED(c);
+        if (c->serial_sums) {
+            k_serial_sum_cells<real><<<1, 32, 0, c->stream>>>(R(c->hecm), N, 1, c->dp.dx, c->d_scal + 0);
+            PFAG_LAUNCHED(c);
+        } else {
+            k_sum_cells<real><<<dim3(RED_BLOCKS, 1), RED_THREADS, 0, c->stream>>>(R(c->hecm), c->ng,
+                                                                                 c->dp.dx * c->dp.dx, c->d_part);
+            PFAG_LAUNCHED(c);
+            k_sum_partials<<<1, 32, 0, c->stream>>>(c->d_part, RED_BLOCKS, c->d_scal + 0);
+            PFAG_LAUNCHED(c);
+        }
         k_lum_ecm_update<real><<<interior_grid(1), dim3(TBX, TBY), 0, c->stream>>>(
             R(c->lum), R(c->ecm), R(c->psi), R(c->hlum), R(c->hecm), R(c->lumn), R(c->ecmn), c->dp, c->d_scal + 0);
         PFAG_LAUNCHED(c);
@@ -881,7 +948,7 @@ struct Plain {
                                         c->stream));
         const real A = (real)c->dp.A_resh, B = (real)c->dp.B_resh;
         const double scale = c->dp.dx * c->dp.dx / (double)c->dp.Ncur;
-        const int nblk = 32;
+        const int nblk = c->serial_sums ? 1 : 32;
         for (;;) {
             k_zone_copy<real><<<zone_grid(), dim3(TBX, TBY), 0, c->stream>>>(R(c->phi), R(c->phin), c->d_xc, c->d_yc,
                                                                              c->N, c->zone, active);
@@ -889,8 +956,13 @@ struct Plain {
             k_cell_relax<real><<<zone_grid(), dim3(TBX, TBY), 0, c->stream>>>(
                 R(c->phi), R(c->phin), R(c->jx), R(c->jy), c->d_xc, c->d_yc, c->N, c->zone, A, B, active);
             PFAG_LAUNCHED(c);
-            k_cell_rdev<real><<<dim3(nblk, Nt), RED_THREADS, 0, c->stream>>>(R(c->phin), R(c->phi), c->d_xc, c->d_yc,
-                                                                             c->N, c->zone, scale, active, c->d_part);
+            if (c->serial_sums)
+                k_serial_cell_rdev<real><<<(Nt + 63) / 64, 64, 0, c->stream>>>(
+                    R(c->phin), R(c->phi), c->d_xc, c->d_yc, c->N, c->zone, Nt, c->dp.dx, (double)c->dp.Ncur, active,
+                    c->d_part);
+            else
+                k_cell_rdev<real><<<dim3(nblk, Nt), RED_THREADS, 0, c->stream>>>(
+                    R(c->phin), R(c->phi), c->d_xc, c->d_yc, c->N, c->zone, scale, active, c->d_part);
             PFAG_LAUNCHED(c);
             PFAG_CUDA_CHECK(cudaMemsetAsync(nact, 0, sizeof(int), c->stream));
             k_cell_check<<<(Nt + 127) / 128, 128, 0, c->stream>>>(c->d_part, nblk, Nt, c->dp.thr_cells, c->p.rimax,

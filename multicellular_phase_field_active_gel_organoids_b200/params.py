@@ -9,9 +9,11 @@ alpha_ECM=0.002, eta_ecm_cells=0.001).
 
 Organoid configurations are in grid units (dx = 1), so the interface width wi,
 the reference radius R0 = R and the target area s0 are rescaled per
-configuration: wi = 1, R0 = R = cell radius, s0 = pi R^2.  With these the
-initial profile 0.5 (1 - tanh((r - R)/2)) = 1 / (1 + exp(r - R)) is the
-reference's own logistic profile (initialisation_functions.cpp:135).
+configuration: wi = sqrt(2), R0 = R = cell radius, s0 = pi R^2.  The
+reshaping relaxation's 1-D equilibrium is a logistic of width wi/sqrt(2), so
+with wi = sqrt(2) the initial profile 0.5 (1 - tanh((r - R)/2)) =
+1 / (1 + exp(r - R)) is that equilibrium (the reference's own logistic
+profile, initialisation_functions.cpp:135).
 """
 from __future__ import annotations
 

@@ -16,13 +16,21 @@ step at which a GPU path takes a different number of reshaping iterations
 than the host, and how far from the loop's threshold the host's rdev was
 there (a decision taken within rounding of the threshold).
 
-Part 2, the 64-cell organoid (1024^2, zone_size 129): the fused FP32 path
-against the fused FP64 path after each of --cfg1-checkpoints steps: per-cell
-area, centroid, perimeter (sum |grad phi| dx, central differences) and rho
-mass (sum rho dx^2), as the largest relative (or absolute, for centroids)
-difference over cells.
+The plain FP64 path runs twice: with its parallel reductions and with the
+serial-order sums (pfag_set_serial_sums: the areas, sum_ecm and the reshaping
+checks' rdev sums taken one thread per sum in the reference's host order), to
+show how far the first reshaping-count difference moves when the summation
+order is the reference's and only the state's rounding differs.
 
-    python tests/long_parity.py --out gpurun_out/long_parity.json
+Part 2, the 64-cell organoid (1024^2, zone_size 129): the fused FP32 path
+after each of --cfg1-checkpoints steps against the plain FP64 path and, at
+the checkpoints tests/golden/long_cfg1.npz holds (the reference's own FP64
+run, 1000 steps), against the reference: per-cell area, centroid, perimeter
+(sum |grad phi| dx, central differences) and rho mass (sum rho dx^2), as the
+largest relative (or absolute, for centroids) difference over cells.  The
+plain FP64 path is compared with the reference at those checkpoints too.
+
+    python tests/long_parity.py --out long_parity.json
 """
 from __future__ import annotations
 
@@ -42,6 +50,7 @@ sys.path.insert(0, ROOT)
 from multicellular_phase_field_active_gel_organoids_b200 import capi  # noqa: E402
 from multicellular_phase_field_active_gel_organoids_b200.params import CONFIGS  # noqa: E402
 from oracle import refrun  # noqa: E402
+from tests.shape import perimeter, rho_mass  # noqa: E402
 
 
 def rel(a, b, mask=None):
@@ -111,14 +120,18 @@ def part1(nsteps: int) -> dict:
     refs[nsteps] = ref
     report = {"config": "cfg0: 256x256, 7 cells R=20, zone_size 65 (box 128)", "steps": nsteps,
               "reference_host_seconds": round(t_ref, 1), "reshaping_threshold": thr, "paths": {}}
-    for name, prec, path in (("plain_f64", 64, capi.PATH_PLAIN), ("fused_f64", 64, capi.PATH_FUSED),
-                             ("fused_f32", 32, capi.PATH_FUSED)):
+    for name, prec, path, serial in (("plain_f64", 64, capi.PATH_PLAIN, False),
+                                     ("plain_f64_serial_sums", 64, capi.PATH_PLAIN, True),
+                                     ("fused_f64", 64, capi.PATH_FUSED, False),
+                                     ("fused_f32", 32, capi.PATH_FUSED, False)):
         dtype = np.float64 if prec == 64 else np.float32
         rows = {}
         iters = np.zeros_like(host_iters)
         t0 = time.time()
         with capi.Simulation(p, prec, path) as sim:
             sim.set_relax_cap(100000)
+            if serial:
+                sim.set_serial_sums(True)
             sim.upload(*cfg.initial_state(dtype))
             for k in range(nsteps):
                 if k == nsteps - 1:
@@ -148,46 +161,64 @@ def part1(nsteps: int) -> dict:
 
 
 def shape_measures(state, dx: float):
-    phi = np.asarray(state["phi"], np.float64)
-    rho = np.asarray(state["rho"], np.float64)
-    gi = 0.5 * (np.roll(phi, -1, axis=1) - np.roll(phi, 1, axis=1))
-    gj = 0.5 * (np.roll(phi, -1, axis=2) - np.roll(phi, 1, axis=2))
-    perim = np.sqrt(gi * gi + gj * gj).sum(axis=(1, 2)) * dx
-    mass = rho.sum(axis=(1, 2)) * dx * dx
-    return perim, mass
+    return perimeter(state["phi"], dx), rho_mass(state["rho"], dx)
+
+
+def compare(a, b, dx):
+    """Per-cell differences of state `a` against `b` (the reference side)."""
+    pa, ma = shape_measures(a, dx)
+    pb, mb = shape_measures(b, dx)
+    return {
+        "area_rel_max": float(np.max(np.abs(a["s"] - b["s"]) / np.abs(b["s"]))),
+        "centroid_max_abs": int(max(np.max(np.abs(a["xc"] - b["xc"])), np.max(np.abs(a["yc"] - b["yc"])))),
+        "perimeter_rel_max": float(np.max(np.abs(pa - pb) / np.abs(pb))),
+        "rho_mass_rel_max": float(np.max(np.abs(ma - mb) / np.maximum(np.abs(mb), 1e-300))),
+    }
+
+
+def compare_golden(a, gold, c, dx):
+    pa, ma = shape_measures(a, dx)
+    return {
+        "area_rel_max": float(np.max(np.abs(a["s"] - gold[f"s_{c}"]) / np.abs(gold[f"s_{c}"]))),
+        "centroid_max_abs": int(max(np.max(np.abs(a["xc"] - gold[f"xc_{c}"])),
+                                    np.max(np.abs(a["yc"] - gold[f"yc_{c}"])))),
+        "perimeter_rel_max": float(np.max(np.abs(pa - gold[f"perimeter_{c}"]) / np.abs(gold[f"perimeter_{c}"]))),
+        "rho_mass_rel_max": float(np.max(np.abs(ma - gold[f"rho_mass_{c}"]) / np.abs(gold[f"rho_mass_{c}"]))),
+    }
 
 
 def part2(checkpoints) -> dict:
     cfg = CONFIGS["cfg1"]()
     p = cfg.params()
     dx = float(p["dx"])
-    report = {"config": "cfg1: 1024x1024, 64 cells R=24, zone_size 129 (box 256)", "checkpoints": {}}
+    gpath = os.path.join(ROOT, "tests", "golden", "long_cfg1.npz")
+    gold = np.load(gpath) if os.path.exists(gpath) else None
+    gsteps = {int(k.split("_")[1]) for k in gold.files if k.startswith("s_")} if gold is not None else set()
+    report = {"config": "cfg1: 1024x1024, 64 cells R=24, zone_size 129 (box 256)",
+              "reference_checkpoints": sorted(gsteps), "checkpoints": {}}
     sims = {}
     done = 0
     try:
-        for prec in (64, 32):
-            s = capi.Simulation(p, prec, capi.PATH_FUSED)
+        for name, prec, path in (("plain_f64", 64, capi.PATH_PLAIN), ("fused_f32", 32, capi.PATH_FUSED)):
+            s = capi.Simulation(p, prec, path)
             s.set_relax_cap(100000)
             s.upload(*cfg.initial_state(np.float64 if prec == 64 else np.float32))
-            sims[prec] = s
+            sims[name] = s
         for c in checkpoints:
             row = {}
-            for prec, s in sims.items():
+            for name, s in sims.items():
                 t0 = time.time()
                 s.step(done, c - done)
-                row[f"seconds_f{prec}"] = round(time.time() - t0, 2)
+                row[f"seconds_{name}"] = round(time.time() - t0, 2)
             done = c
-            a = gpu_state(sims[64])
-            b = gpu_state(sims[32])
-            pa, ma = shape_measures(a, dx)
-            pb, mb = shape_measures(b, dx)
-            row.update({
-                "area_rel_max": float(np.max(np.abs(b["s"] - a["s"]) / np.abs(a["s"]))),
-                "centroid_max_abs": int(max(np.max(np.abs(b["xc"] - a["xc"])), np.max(np.abs(b["yc"] - a["yc"])))),
-                "perimeter_rel_max": float(np.max(np.abs(pb - pa) / np.abs(pa))),
-                "rho_mass_rel_max": float(np.max(np.abs(mb - ma) / np.maximum(np.abs(ma), 1e-300))),
-                "phi_linf": float(np.max(np.abs(np.asarray(b["phi"], np.float64) - a["phi"]))),
-            })
+            a = gpu_state(sims["plain_f64"])
+            b = gpu_state(sims["fused_f32"])
+            row["fused_f32_vs_plain_f64"] = compare(b, a, dx)
+            row["fused_f32_vs_plain_f64"]["phi_linf"] = float(np.max(np.abs(np.asarray(b["phi"], np.float64)
+                                                                             - a["phi"])))
+            if c in gsteps:
+                row["fused_f32_vs_reference"] = compare_golden(b, gold, c, dx)
+                row["plain_f64_vs_reference"] = compare_golden(a, gold, c, dx)
             report["checkpoints"][str(c)] = row
             print(c, row, flush=True)
     except capi.PfagError as e:
@@ -212,7 +243,7 @@ def main() -> int:
         with open(a.out, "w") as f:
             json.dump(out, f, indent=1)
     if not a.skip_cfg1:
-        out["cfg1_f32_vs_f64"] = part2([int(x) for x in a.cfg1_checkpoints.split(",")])
+        out["cfg1_f32"] = part2([int(x) for x in a.cfg1_checkpoints.split(",")])
     with open(a.out, "w") as f:
         json.dump(out, f, indent=1)
     print(json.dumps(out, indent=1))
