@@ -215,7 +215,9 @@ int pfag_fn_copy_back(pfag_ctx *ctx);                          /* run_with_activ
  * caller owns; the work is enqueued on `stream` (a cudaStream_t, NULL for the
  * default stream) and not synchronised.  The first call on a device resolves
  * the scratch address there (cudaGetSymbolAddress) and should be made before
- * any stream capture.  All calls share the one scratch array, so calls that
+ * any stream capture.  The resolved address belongs to the device's current
+ * primary context: a process that resets the device (cudaDeviceReset) must
+ * not call this entry point on that device afterwards.  All calls share the one scratch array, so calls that
  * overlap on the GPU (different streams, no ordering) race; order them on one
  * stream.  Every scratch value a call reads it first writes, so no clearing
  * is needed between calls. */

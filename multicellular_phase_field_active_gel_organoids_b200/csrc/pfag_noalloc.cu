@@ -22,7 +22,9 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 // 1024 cells x 128 partials x 8 bytes = 1 MiB per device.
 static __device__ __align__(256) double g_area_partials[NOALLOC_MAX_CELLS * NOALLOC_BLOCKS];
 
-// Device addresses of g_area_partials, resolved once per device.
+// Device addresses of g_area_partials, resolved once per device (valid for
+// the life of the device's primary context: a cudaDeviceReset reloads the
+// module, and the entry point must not be called on that device again).
 double *g_partials_addr[NOALLOC_MAX_DEVICES] = {};
 std::mutex g_setup_mu;
 
