@@ -167,8 +167,17 @@ def coarse_config(fine: OrganoidConfig) -> OrganoidConfig:
 
 
 def fine_config(ncells: int, seed: int, N: int = 1024, zone_size: int = 129) -> OrganoidConfig:
-    """A seeded fine organoid of the cfg1 family (R = 24, jittered hexagonal lattice)."""
-    return jittered_hex_organoid(name=f"fine{seed}", N=N, ncells=ncells, zone_size=zone_size, seed=seed)
+    """A seeded fine organoid of the cfg1 family (R = 24, jittered hexagonal
+    lattice), its lattice clipped so that every zone stays on the grid; the
+    cell count is capped at what that circle holds."""
+    clip = min(220.0, N / 2.0 - zone_size - 4.0)
+    for n in range(ncells, 0, -1):
+        try:
+            return jittered_hex_organoid(name=f"fine{seed}", N=N, ncells=n, zone_size=zone_size, seed=seed,
+                                         clip=clip)
+        except ValueError:
+            continue
+    raise ValueError(f"no lattice point within {clip} of the centre")
 
 
 def _field(sim, name):

@@ -231,7 +231,7 @@ extern "C" int pfag_download(pfag_ctx *c, void *phi, void *rho, void *lum, void 
     return PFAG_OK;
 }
 
-static int fetch_observables(pfag_ctx *c) {
+int pfag_fetch_observables(pfag_ctx *c) {
     PFAG_CUDA_CHECK(cudaMemcpyAsync(c->h_s, c->d_s, sizeof(double) * c->Ntot, cudaMemcpyDeviceToHost, c->stream));
     PFAG_CUDA_CHECK(cudaMemcpyAsync(c->h_f0, c->d_f0, sizeof(double) * c->Ntot, cudaMemcpyDeviceToHost, c->stream));
     PFAG_CUDA_CHECK(cudaMemcpyAsync(c->h_xc, c->d_xc, sizeof(int) * c->Ntot, cudaMemcpyDeviceToHost, c->stream));
@@ -250,7 +250,7 @@ static int run_steps(pfag_ctx *c, int it0, int nsteps, bool sync) {
     if (sync) {
         PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
         PFAG_TRY(pfag_check_device_error(c));
-        PFAG_TRY(fetch_observables(c));
+        PFAG_TRY(pfag_fetch_observables(c));
     }
     return PFAG_OK;
 }
@@ -261,7 +261,7 @@ extern "C" int pfag_sync(pfag_ctx *c) {
     if (!c) return PFAG_E_ARG;
     PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
     PFAG_TRY(pfag_check_device_error(c));
-    return fetch_observables(c);
+    return pfag_fetch_observables(c);
 }
 
 extern "C" int pfag_observables_async(pfag_ctx *c, double *s, double *f0, int *xc, int *yc) {
@@ -409,7 +409,7 @@ extern "C" int pfag_fn_reshaping_lumen_or_ECM(pfag_ctx *c, int which) {
 extern "C" int pfag_fn_sum_s_kernels(pfag_ctx *c, double *s_host, double *f0_host) {
     PFAG_TRY(need_plain(c));
     PFAG_TRY(pfag_plain_fn(c, "sum_s", 0));
-    PFAG_TRY(fetch_observables(c));
+    PFAG_TRY(pfag_fetch_observables(c));
     return pfag_get_areas(c, s_host, f0_host);
 }
 
@@ -417,7 +417,7 @@ extern "C" int pfag_generate_initial(pfag_ctx *c, double rho0, double tol, int m
     PFAG_TRY(need_plain(c));
     if (!(tol > 0.0) || !(rho0 >= 0.0)) { pfag_set_error("rho0 must be >= 0 and tol > 0"); return PFAG_E_ARG; }
     PFAG_TRY(pfag_plain_generate(c, rho0, tol, make_fields));
-    return fetch_observables(c);
+    return pfag_fetch_observables(c);
 }
 
 extern "C" int pfag_fn_saving_out_functions(pfag_ctx *c, void *phi_out, void *rho_out, void *lum_out, void *ecm_out) {

@@ -129,28 +129,28 @@ struct Blue {
         for (int q = 0; q < E1; q++) {
             const int n = idx(t, q);
             if (n < M) {
-                cx c = __ldg(&tb.cw[n]);
+                cx c = tb.cw[n];
                 if (!INV) c = cconj(c);
                 v[q] = cmul(v[q], c);
             } else {
                 v[q] = CxOps<cx>::mk((real)0.0, (real)0.0);
             }
         }
-        RF::template run<false>(v, t, sm, tw);
+        RF::template run<false, true>(v, t, sm, tw);
 #pragma unroll
         for (int p = 0; p < E1; p++) {
-            cx w = __ldg(&tb.wf[RF::out_index(t, p / TT, p % TT)]);
+            cx w = tb.wf[RF::out_index(t, p / TT, p % TT)];
             if (INV) w = cconj(w);
             v[p] = cmul(v[p], w);
         }
         to_in(v);
-        RF::template run<true>(v, t, sm, tw);
+        RF::template run<true, true>(v, t, sm, tw);
         to_in(v);
 #pragma unroll
         for (int q = 0; q < E1; q++) {
             const int n = idx(t, q);
             if (n < M) {
-                cx c = __ldg(&tb.cw[n]);
+                cx c = tb.cw[n];
                 if (!INV) c = cconj(c);
                 v[q] = cmul(v[q], c);
             }
@@ -164,15 +164,15 @@ struct Blue {
 #pragma unroll
         for (int q = 0; q < E1; q++)
             if (idx(t, q) >= M) v[q] = CxOps<cx>::mk((real)0.0, (real)0.0);
-        RF::template run<false>(v, t, sm, tw);
+        RF::template run<false, true>(v, t, sm, tw);
 #pragma unroll
         for (int p = 0; p < E1; p++) {
-            const real hi = __ldg(&tb.hdi[RF::out_index(t, p / TT, p % TT)]);   // times i hi
+            const real hi = tb.hdi[RF::out_index(t, p / TT, p % TT)];   // times i hi
             const cx x = v[p];
             v[p] = CxOps<cx>::mk(-x.y * hi, x.x * hi);
         }
         to_in(v);
-        RF::template run<true>(v, t, sm, tw);
+        RF::template run<true, true>(v, t, sm, tw);
         to_in(v);
     }
 };
@@ -186,9 +186,64 @@ template <typename real, int L> struct BlueGeom {
     static constexpr int MINB = sizeof(real) == 4 ? 2 : 1;
 };
 
-template <typename cx>
-__device__ __forceinline__ void load_tw(cx *tw, const cx *__restrict__ g, int L) {
-    for (int k = threadIdx.x; k < L; k += blockDim.x) tw[k] = g[k];
+// global -> shared copy of one 8- or 16-byte element, asynchronous (cp.async);
+// blue_cp_wait waits for the calling thread's copies
+template <typename T>
+__device__ __forceinline__ void blue_cp(T *dst, const T *src) {
+    static_assert(sizeof(T) == 8 || sizeof(T) == 16, "element size");
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(sizeof(T)) : "memory");
+}
+__device__ __forceinline__ void blue_cp_wait() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// the twiddles of the length-L register FFT in its [E1][TT] layout, from the
+// natural-order table g[k] = exp(-2 pi i k / L)
+template <typename cx, int L>
+__device__ __forceinline__ void load_tw(cx *tw, const cx *__restrict__ g) {
+    constexpr int TT = RegFFT<cx, L>::TT;
+    for (int e = threadIdx.x; e < L; e += blockDim.x) {
+        const int k1 = e / TT, t = e - k1 * TT;
+        tw[e] = g[(t * k1) & (L - 1)];
+    }
+}
+
+// The kernels' copy of the tables in shared memory at `base` (after the
+// twiddles): the chirp (M) and its kernel's spectrum (L) when `chirp`, the
+// derivative kernel's spectrum (L reals) when `deriv`; returns the table set
+// the transforms read and the first byte after it.
+template <typename cx, int L>
+__device__ __forceinline__ BlueTabs<cx> stage_tabs(const BlueTabs<cx> &g, unsigned char *base, int M, bool chirp,
+                                                   bool deriv, unsigned char **end) {
+    typedef typename CxOps<cx>::real real;
+    BlueTabs<cx> s = g;
+    cx *p = reinterpret_cast<cx *>(base);
+    if (chirp) {
+        cx *wf = p, *cw = p + L;           // wf [L], then cw [M] (rounded up to even)
+        for (int e = threadIdx.x; e < L; e += blockDim.x) {
+            wf[e] = g.wf[e];
+            if (e < M) cw[e] = g.cw[e];
+        }
+        s.wf = wf;
+        s.cw = cw;
+        p += L + ((M + 1) & ~1);
+    }
+    real *h = reinterpret_cast<real *>(p);
+    if (deriv) {
+        for (int e = threadIdx.x; e < L; e += blockDim.x) h[e] = g.hdi[e];
+        s.hdi = h;
+        h += L;
+    }
+    *end = reinterpret_cast<unsigned char *>(h);
+    return s;
+}
+
+// bytes stage_tabs takes
+template <typename cx, int L>
+constexpr size_t tabs_bytes(int M, bool chirp, bool deriv) {
+    return (chirp ? ((size_t)L + (size_t)((M + 1) & ~1)) * sizeof(cx) : 0) +
+           (deriv ? (size_t)L * sizeof(typename CxOps<cx>::real) : 0);
 }
 
 // Pass A' (rows, forward): tasks [0, M) of a cell transform row i of Y1
@@ -206,7 +261,10 @@ kbl_rowsA(typename Cplx<real>::type *__restrict__ Y1, const real *__restrict__ Y
     cx *tw = (cx *)smraw;
     const int t = threadIdx.x % TT, g = threadIdx.x / TT;
     cx *sm = tw + L + (size_t)g * L;
-    load_tw(tw, tb.tw, L);
+    load_tw<cx, L>(tw, tb.tw);
+    unsigned char *end;
+    const BlueTabs<cx> st = stage_tabs<cx, L>(tb, reinterpret_cast<unsigned char *>(tw + L + (size_t)GPB * L), M,
+                                              true, false, &end);
     __syncthreads();
     const int per = M + M / 2, H = M / 2 + 1;
     const long total = (long)Ntot * per;
@@ -234,7 +292,7 @@ kbl_rowsA(typename Cplx<real>::type *__restrict__ Y1, const real *__restrict__ Y
                 v[q] = (live && j < M) ? CxOps<cx>::mk(ra[j], ra[j + M]) : CxOps<cx>::mk((real)0.0, (real)0.0);
             }
         }
-        B::template dft<false>(v, t, M, sm, tw, tb);
+        B::template dft<false>(v, t, M, sm, tw, st);
         if (!pair) {
             if (live) {
                 cx *dst = Y1 + ((size_t)n * M + a) * M;
@@ -279,8 +337,9 @@ struct ColSet {
 
 // Column transforms (forward, or inverse with INV) of up to two column sets;
 // a block stages GPB columns of one cell in shared memory (one slot of L + 1
-// complex per column, which is also the exchange scratch of its transform),
-// transforms them and stores them back.
+// complex per column, which is also the exchange scratch of its transform;
+// all of a thread's copies in flight at once), transforms them and stores
+// them back.
 template <typename real, int L, bool INV>
 __global__ void __launch_bounds__(BlueGeom<real, L>::THREADS, BlueGeom<real, L>::MINB)
 kbl_cols(ColSet<typename Cplx<real>::type> s0, ColSet<typename Cplx<real>::type> s1, int M, int Ntot,
@@ -292,7 +351,10 @@ kbl_cols(ColSet<typename Cplx<real>::type> s0, ColSet<typename Cplx<real>::type>
     cx *tw = (cx *)smraw;
     cx *Z = tw + L;                       // [GPB][S]
     const int t = threadIdx.x % TT, g = threadIdx.x / TT;
-    load_tw(tw, tb.tw, L);
+    load_tw<cx, L>(tw, tb.tw);
+    unsigned char *end;
+    const BlueTabs<cx> st = stage_tabs<cx, L>(tb, reinterpret_cast<unsigned char *>(Z + (size_t)GPB * S), M, true,
+                                              false, &end);
     const long per = (long)s0.nblk + s1.nblk;
     const long total = (long)Ntot * per;
     for (long task = blockIdx.x; task < total; task += gridDim.x) {
@@ -301,11 +363,12 @@ kbl_cols(ColSet<typename Cplx<real>::type> s0, ColSet<typename Cplx<real>::type>
         const int c0 = ((b < s0.nblk) ? b : b - s0.nblk) * GPB;
         const int nc = min(GPB, cs.ncol - c0);
         cx *src = cs.base + (size_t)n * cs.cell_stride + c0;
-        __syncthreads();                  // the previous task's stores have read Z
+        __syncthreads();                  // the previous task's stores have read Z (and the tables are staged)
         for (int e = threadIdx.x; e < M * nc; e += blockDim.x) {
             const int i = e / nc, c = e - i * nc;
-            Z[(size_t)c * S + i] = src[(size_t)i * cs.stride + c];
+            blue_cp(Z + (size_t)c * S + i, src + (size_t)i * cs.stride + c);
         }
+        blue_cp_wait();
         __syncthreads();
         {
             cx *col = Z + (size_t)g * S;
@@ -316,7 +379,7 @@ kbl_cols(ColSet<typename Cplx<real>::type> s0, ColSet<typename Cplx<real>::type>
                 v[q] = (g < nc && i < M) ? col[i] : CxOps<cx>::mk((real)0.0, (real)0.0);
             }
             __syncwarp();
-            B::template dft<INV>(v, t, M, col, tw, tb);
+            B::template dft<INV>(v, t, M, col, tw, st);
 #pragma unroll
             for (int q = 0; q < E1; q++) {
                 const int i = B::idx(t, q);
@@ -349,8 +412,12 @@ kbl_rowsD(const typename Cplx<real>::type *__restrict__ Y1, real *__restrict__ X
     cx *tw = (cx *)smraw;
     const int t = threadIdx.x % TT, g = threadIdx.x / TT;
     cx *sm = tw + L + (size_t)g * L;
-    real *fys = reinterpret_cast<real *>(tw + L + (size_t)GPB * L) + (size_t)g * 2 * M;   // Fy of the two rows
-    load_tw(tw, tb.tw, L);
+    real *fys0 = reinterpret_cast<real *>(tw + L + (size_t)GPB * L);
+    real *fys = fys0 + (size_t)g * 2 * M;   // Fy of the two rows
+    load_tw<cx, L>(tw, tb.tw);
+    unsigned char *end;
+    const BlueTabs<cx> st = stage_tabs<cx, L>(tb, reinterpret_cast<unsigned char *>(fys0 + (size_t)GPB * 2 * M), M,
+                                              true, true, &end);
     __syncthreads();
     const int per = M / 2;
     const long total = (long)Ntot * per;
@@ -370,7 +437,7 @@ kbl_rowsD(const typename Cplx<real>::type *__restrict__ Y1, real *__restrict__ X
                 const int j = B::idx(t, q);
                 v[q] = (live && j < M) ? Y1[rowo + j] : CxOps<cx>::mk((real)0.0, (real)0.0);
             }
-            B::template dft<true>(v, t, M, sm, tw, tb);
+            B::template dft<true>(v, t, M, sm, tw, st);
             const real *rh = rho + (size_t)n * N * N + (size_t)(bi + i) * N + bj;
 #pragma unroll
             for (int q = 0; q < E1; q++) {
@@ -393,7 +460,7 @@ kbl_rowsD(const typename Cplx<real>::type *__restrict__ Y1, real *__restrict__ X
             const int j = B::idx(t, q);
             v[q] = (j < M) ? CxOps<cx>::mk(fys[j], fys[M + j]) : CxOps<cx>::mk((real)0.0, (real)0.0);
         }
-        B::deriv(v, t, M, sm, tw, tb);
+        B::deriv(v, t, M, sm, tw, st);
         if (live) {
             real *d0 = X + (size_t)Ntot * M * M + ((size_t)n * M + i0) * M;
 #pragma unroll
@@ -421,7 +488,10 @@ kbl_colsE(const real *__restrict__ X, real *__restrict__ rho, const real *__rest
     cx *tw = (cx *)smraw;
     cx *Z = tw + L;                       // [GPB][S]: column pairs
     const int t = threadIdx.x % TT, g = threadIdx.x / TT;
-    load_tw(tw, tb.tw, L);
+    load_tw<cx, L>(tw, tb.tw);
+    unsigned char *end;
+    const BlueTabs<cx> st = stage_tabs<cx, L>(tb, reinterpret_cast<unsigned char *>(Z + (size_t)GPB * S), M, false,
+                                              true, &end);
     const int nblk = (M / 2 + GPB - 1) / GPB;
     const long total = (long)Ntot * nblk;
     const real dtr = (real)dt;
@@ -432,8 +502,9 @@ kbl_colsE(const real *__restrict__ X, real *__restrict__ rho, const real *__rest
         __syncthreads();
         for (int e = threadIdx.x; e < M * np; e += blockDim.x) {
             const int i = e / np, p = e - i * np;
-            Z[(size_t)p * S + i] = *reinterpret_cast<const cx *>(fx + (size_t)i * M + 2 * (p0 + p));
+            blue_cp(Z + (size_t)p * S + i, reinterpret_cast<const cx *>(fx + (size_t)i * M + 2 * (p0 + p)));
         }
+        blue_cp_wait();
         __syncthreads();
         {
             cx *col = Z + (size_t)g * S;
@@ -444,7 +515,7 @@ kbl_colsE(const real *__restrict__ X, real *__restrict__ rho, const real *__rest
                 v[q] = (g < np && i < M) ? col[i] : CxOps<cx>::mk((real)0.0, (real)0.0);
             }
             __syncwarp();
-            B::deriv(v, t, M, col, tw, tb);
+            B::deriv(v, t, M, col, tw, st);
 #pragma unroll
             for (int q = 0; q < E1; q++) {
                 const int i = B::idx(t, q);
@@ -456,13 +527,29 @@ kbl_colsE(const real *__restrict__ X, real *__restrict__ rho, const real *__rest
         real *rcell = rho + (size_t)n * N * N;
         const real *rb = Rb + (size_t)n * M * M, *dy = X + (size_t)Ntot * M * M + (size_t)n * M * M;
         const int ncols = 2 * np;
-        for (int e = threadIdx.x; e < M * ncols; e += blockDim.x) {
-            const int i = e / ncols, cc = e - i * ncols;
-            const int p = cc >> 1, col = 2 * p0 + cc;
-            const cx w = Z[(size_t)p * S + i];
-            const size_t bo = (size_t)i * M + col;
-            real &ro = rcell[(size_t)(bi + i) * N + bj + col];
-            ro = ro + dtr * rb[bo] + ((cc & 1 ? w.y : w.x) + dy[bo]);
+        constexpr int U = 4;              // four sites' loads in flight per thread
+        for (int e0 = threadIdx.x; e0 < M * ncols; e0 += U * blockDim.x) {
+            real ro[U], rr[U], yy[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int e = e0 + u * blockDim.x;
+                if (e < M * ncols) {
+                    const int i = e / ncols, cc = e - i * ncols, col = 2 * p0 + cc;
+                    const size_t bo = (size_t)i * M + col;
+                    ro[u] = rcell[(size_t)(bi + i) * N + bj + col];
+                    rr[u] = rb[bo];
+                    yy[u] = dy[bo];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int e = e0 + u * blockDim.x;
+                if (e < M * ncols) {
+                    const int i = e / ncols, cc = e - i * ncols, col = 2 * p0 + cc;
+                    const cx w = Z[(size_t)(cc >> 1) * S + i];
+                    rcell[(size_t)(bi + i) * N + bj + col] = ro[u] + dtr * rr[u] + ((cc & 1 ? w.y : w.x) + yy[u]);
+                }
+            }
         }
     }
 }

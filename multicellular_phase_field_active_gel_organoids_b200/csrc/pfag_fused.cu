@@ -184,6 +184,7 @@ extern "C" int pfag_batch_sync(pfag_batch *b) {
         PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
         PFAG_TRY(pfag_check_device_error(c));
         PFAG_TRY(c->prec == 64 ? pfag_fused_stats_f64(c) : pfag_fused_stats_f32(c));
+        PFAG_TRY(pfag_fetch_observables(c));
     }
     return PFAG_OK;
 }

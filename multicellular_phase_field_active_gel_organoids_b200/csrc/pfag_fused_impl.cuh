@@ -868,7 +868,7 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) kr_boxA(const 
             cp_async_elem(xys + e, rs + (size_t)r * N + cc);
         }
     }
-    fft_twiddles(tw, M);
+    RegFFT<cx, M>::twiddles_kt(tw);
     cp_async_wait_all();
     __syncthreads();
     const size_t rowo = ((size_t)n * M + i) * M;
@@ -892,7 +892,7 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) kr_boxA(const 
         v[q].y = yy;
     }
     __syncthreads();    // every group is done with the staged phi before scr becomes exchange space
-    RF::template run<false>(v, t, scr + g * M, tw);
+    RF::template run<false, true>(v, t, scr + g * M, tw);
 #pragma unroll
     for (int r = 0; r < RF::R2; r++)
 #pragma unroll
@@ -902,7 +902,7 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) kr_boxA(const 
         v[q].x = xys[g * M + RF::in_index(t, q)];
         v[q].y = (real)0.0;
     }
-    RF::template run<false>(v, t, scr + g * M, tw);
+    RF::template run<false, true>(v, t, scr + g * M, tw);
 #pragma unroll
     for (int r = 0; r < RF::R2; r++)
 #pragma unroll
@@ -939,7 +939,7 @@ __device__ __forceinline__ void columns_fft(cx *Z, int nseq_pad, const cx *tw) {
 #pragma unroll
             for (int q = 0; q < E1; q++) v[q] = col[RF::in_index(t, q)];
             __syncwarp();
-            RF::template run<INV>(v, t, col, tw);
+            RF::template run<INV, true>(v, t, col, tw);
 #pragma unroll
             for (int r = 0; r < RF::R2; r++)
 #pragma unroll
@@ -1009,7 +1009,7 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxC2(const
     extern __shared__ unsigned char smraw[];
     cx *tw = (cx *)smraw;
     cx *scr = tw + M;
-    fft_twiddles(tw, M);
+    RegFFT<cx, M>::twiddles_kt(tw);
     __syncthreads();
     const int t = threadIdx.x % TT, g = threadIdx.x / TT;
     const int n = blockIdx.y, i = blockIdx.x * ROWS + g;
@@ -1021,7 +1021,7 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxC2(const
     cx v[E1];
 #pragma unroll
     for (int q = 0; q < E1; q++) v[q] = Y1[rowo + RF::in_index(t, q)];
-    RF::template run<true>(v, t, sm, tw);
+    RF::template run<true, true>(v, t, sm, tw);
     const real mm = (real)((double)M * (double)M);
     const real *rh = rho + (size_t)n * N * N + (size_t)(bi + i) * N + bj;
 #pragma unroll
@@ -1042,7 +1042,7 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxC2(const
 #pragma unroll
     for (int q = 0; q < E1; q++) v[q] = sm[RF::in_index(t, q)];
     __syncwarp();
-    RF::template run<false>(v, t, sm, tw);
+    RF::template run<false, true>(v, t, sm, tw);
     // times -i jr, Nyquist bin zero
 #pragma unroll
     for (int r = 0; r < RF::R2; r++)
@@ -1060,7 +1060,7 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) kr_boxC2(const
 #pragma unroll
     for (int q = 0; q < E1; q++) v[q] = sm[RF::in_index(t, q)];
     __syncwarp();
-    RF::template run<true>(v, t, sm, tw);
+    RF::template run<true, true>(v, t, sm, tw);
     const real dtk = (real)(a.dt * a.kfac), inv_m = (real)(1.0 / (double)M);
 #pragma unroll
     for (int r = 0; r < RF::R2; r++)
@@ -1088,7 +1088,7 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) kr_boxD2(const
     extern __shared__ unsigned char smraw[];
     cx *tw = (cx *)smraw;
     cx *Z = tw + M;                                   // [NSP][S]
-    fft_twiddles(tw, M);
+    RegFFT<cx, M>::twiddles_kt(tw);
     const int n = blockIdx.y, c0 = blockIdx.x * COLS;
     const int N = a.N;
     const real *fx = X + (size_t)n * M * M, *dy = X + (size_t)a.Ntot * M * M + (size_t)n * M * M;
@@ -1169,7 +1169,7 @@ __global__ void __launch_bounds__(BT, 1280 / BT) kr_boxB(typename Cplx<real>::ty
     constexpr int S = M + 1, WG = BoxGeom<M>::WG;
     extern __shared__ unsigned char smraw[];
     cx *tw = (cx *)smraw;
-    fft_twiddles(tw, M);
+    RegFFT<cx, M>::twiddles_kt(tw);
     __shared__ ColSlots cs;
     const int n = blockIdx.y;
     if (threadIdx.x == 0) make_slots(cs, blockIdx.x * G, G, M);
@@ -2688,14 +2688,17 @@ struct Fused {
         cx *Y1 = (cx *)r->Y1, *Y2 = (cx *)r->Y2, *Hs = (cx *)r->Gsp;
         const BlueTabs<cx> tb = blue_tabs();
         const size_t cs = sizeof(cx);
-        const size_t sm_rows = (size_t)(1 + BGm::GPB) * L * cs;
-        const size_t sm_cols = ((size_t)L + (size_t)BGm::GPB * (L + 1)) * cs;
+        const size_t tab_c = tabs_bytes<cx, L>(M, true, false), tab_d = tabs_bytes<cx, L>(M, false, true);
+        const size_t sm_rows = (size_t)(1 + BGm::GPB) * L * cs + tab_c;
+        const size_t sm_rowsD = (size_t)(1 + BGm::GPB) * L * cs + (size_t)BGm::GPB * 2 * M * sizeof(real) +
+                                tabs_bytes<cx, L>(M, true, true);
+        const size_t sm_cols = ((size_t)L + (size_t)BGm::GPB * (L + 1)) * cs + tab_c;
+        const size_t sm_colsE = ((size_t)L + (size_t)BGm::GPB * (L + 1)) * cs + tab_d;
         PFAG_TRY(smem_at_least((const void *)kbl_rowsA<real, L>, sm_rows));
-        const size_t sm_rowsD = sm_rows + (size_t)BGm::GPB * 2 * M * sizeof(real);
         PFAG_TRY(smem_at_least((const void *)kbl_rowsD<real, L>, sm_rowsD));
         PFAG_TRY(smem_at_least((const void *)kbl_cols<real, L, false>, sm_cols));
         PFAG_TRY(smem_at_least((const void *)kbl_cols<real, L, true>, sm_cols));
-        PFAG_TRY(smem_at_least((const void *)kbl_colsE<real, L>, sm_cols));
+        PFAG_TRY(smem_at_least((const void *)kbl_colsE<real, L>, sm_colsE));
         const dim3 g((M * M + 255) / 256, Nt);
         pfag_prof_begin(c, "kg_stress");
         kg_stress<real><<<g, 256, 0, s>>>(R(c->phi), R(c->rho), R(c->lum), R(c->ecm), c->d_xc, c->d_yc, ba, Y1, Y2,
@@ -2736,7 +2739,7 @@ struct Fused {
         {
             const long tasks = (long)Nt * ((M / 2 + BGm::GPB - 1) / BGm::GPB);
             pfag_prof_begin(c, "kbl_colsE");
-            kbl_colsE<real, L><<<(unsigned)tasks, BGm::THREADS, sm_cols, s>>>(X, R(c->rho), R(r->Rb), c->d_xc,
+            kbl_colsE<real, L><<<(unsigned)tasks, BGm::THREADS, sm_colsE, s>>>(X, R(c->rho), R(r->Rb), c->d_xc,
                                                                               c->d_yc, N, z, M, Nt, c->dp.dt, tb);
             PFAG_LAUNCHED(c);
         }

@@ -144,8 +144,10 @@ struct RegFFT {
     // exchange layout: row k1 of TT entries, columns swizzled by k1
     static __device__ __forceinline__ int sidx(int k1, int t) { return k1 * TT + (t ^ (k1 & (TT - 1))); }
 
-    // sm: M complex of shared memory private to the group; tw[k] = exp(-2 pi i k / M)
-    template <bool INV>
+    // sm: M complex of shared memory private to the group; tw[k] = exp(-2 pi i k / M),
+    // or with KT the same values laid out as [E1][TT]: tw[k1 TT + t] = exp(-2 pi i t k1 / M)
+    // (a warp's twiddle loads then hit distinct banks whatever k1 is)
+    template <bool INV, bool KT = false>
     static __device__ __forceinline__ void run(T (&v)[E1], int t, T *sm, const T *tw) {
         dft_dif<E1, INV>(v);
 #pragma unroll
@@ -153,7 +155,7 @@ struct RegFFT {
             const int k1 = brev_c(p, ilog2_c(E1));
             T x = v[p];
             if (k1 != 0) {
-                T w = tw[(t * k1) & (M - 1)];
+                T w = KT ? tw[k1 * TT + t] : tw[(t * k1) & (M - 1)];
                 if (INV) w = cconj(w);
                 x = cmul(x, w);
             }
@@ -171,6 +173,26 @@ struct RegFFT {
             for (int p = 0; p < TT; p++) v[r * TT + brev_c(p, ilog2_c(TT))] = u[p];
         }
         __syncwarp();
+    }
+
+    // the twiddle table in the [E1][TT] layout of run<INV, true>, computed as
+    // fft_twiddles computes the natural-order one (the same values)
+    static __device__ __forceinline__ void twiddles_kt(T *tw) {
+        typedef typename CxOps<T>::real real;
+        for (int e = threadIdx.x; e < M; e += blockDim.x) {
+            const int k1 = e / TT, t = e - k1 * TT, k = (t * k1) & (M - 1);
+            real s, c;
+            if (sizeof(real) == 8) {
+                double sd, cd;
+                sincospi(-2.0 * (double)k / (double)M, &sd, &cd);
+                s = (real)sd; c = (real)cd;
+            } else {
+                float sf, cf;
+                sincospif(-2.0f * (float)k / (float)M, &sf, &cf);
+                s = (real)sf; c = (real)cf;
+            }
+            tw[e] = CxOps<T>::mk(c, s);
+        }
     }
 
     // natural index of the output held in v[r*TT + k2] by thread t
