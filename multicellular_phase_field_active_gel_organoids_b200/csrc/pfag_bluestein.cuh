@@ -397,14 +397,15 @@ kbl_cols(ColSet<typename Cplx<real>::type> s0, ColSet<typename Cplx<real>::type>
 // Pass D' (rows, inverse): for rows i, i+1 of a cell, the inverse row
 // transforms of Y1 give M^2 (vx + i vy); Fx = rho vx / M^2 is stored in X
 // (plane 0, row-major) for the column pass, and Fy = rho vy / M^2 of the two
-// rows is differentiated along the row at once (one complex convolution),
-// the results (dt kfac folded in) stored in plane 1 (load_fft_rho_v and the
-// row half of update_fft_rho, rho_functions.cpp:213-284).
+// rows is differentiated along the row at once (one complex convolution);
+// plane 1 receives dt R + that row term (dt kfac folded in) (load_fft_rho_v
+// and the row half of update_fft_rho, rho_functions.cpp:213-284).
 template <typename real, int L>
 __global__ void __launch_bounds__(BlueGeom<real, L>::THREADS, BlueGeom<real, L>::MINB)
 kbl_rowsD(const typename Cplx<real>::type *__restrict__ Y1, real *__restrict__ X, const real *__restrict__ rho,
-          const int *__restrict__ xc, const int *__restrict__ yc, int N, int z, int M, int Ntot,
-          BlueTabs<typename Cplx<real>::type> tb, real *__restrict__ vdx, real *__restrict__ vdy) {
+          const real *__restrict__ Rb, double dt, const int *__restrict__ xc, const int *__restrict__ yc, int N,
+          int z, int M, int Ntot, BlueTabs<typename Cplx<real>::type> tb, real *__restrict__ vdx,
+          real *__restrict__ vdy) {
     typedef typename Cplx<real>::type cx;
     typedef Blue<cx, L> B;
     constexpr int TT = B::TT, E1 = B::E1, GPB = BlueGeom<real, L>::GPB;
@@ -463,24 +464,25 @@ kbl_rowsD(const typename Cplx<real>::type *__restrict__ Y1, real *__restrict__ X
         B::deriv(v, t, M, sm, tw, st);
         if (live) {
             real *d0 = X + (size_t)Ntot * M * M + ((size_t)n * M + i0) * M;
+            const real *r0 = Rb + ((size_t)n * M + i0) * M;
+            const real dtr = (real)dt;
 #pragma unroll
             for (int q = 0; q < E1; q++) {
                 const int j = B::idx(t, q);
-                if (j < M) { d0[j] = v[q].x; d0[M + j] = v[q].y; }
+                if (j < M) {
+                    d0[j] = dtr * r0[j] + v[q].x;
+                    d0[M + j] = dtr * r0[M + j] + v[q].y;
+                }
             }
         }
     }
 }
 
 // Pass E' (columns): two real columns of Fx per complex sequence, the
-// derivative along the column (dt kfac folded in), then the new rho =
-// rho + dt R + column term + row term on the box, in place (update_fft_rho
-// and copy_to_rhon, rho_functions.cpp:213-265, by linearity).
+// derivative along the column (dt kfac folded in) stored over Fx in plane 0.
 template <typename real, int L>
 __global__ void __launch_bounds__(BlueGeom<real, L>::THREADS, BlueGeom<real, L>::MINB)
-kbl_colsE(const real *__restrict__ X, real *__restrict__ rho, const real *__restrict__ Rb,
-          const int *__restrict__ xc, const int *__restrict__ yc, int N, int z, int M, int Ntot, double dt,
-          BlueTabs<typename Cplx<real>::type> tb) {
+kbl_colsE(real *__restrict__ X, int M, int Ntot, BlueTabs<typename Cplx<real>::type> tb) {
     typedef typename Cplx<real>::type cx;
     typedef Blue<cx, L> B;
     constexpr int TT = B::TT, E1 = B::E1, GPB = BlueGeom<real, L>::GPB, S = L + 1;
@@ -494,15 +496,14 @@ kbl_colsE(const real *__restrict__ X, real *__restrict__ rho, const real *__rest
                                               true, &end);
     const int nblk = (M / 2 + GPB - 1) / GPB;
     const long total = (long)Ntot * nblk;
-    const real dtr = (real)dt;
     for (long task = blockIdx.x; task < total; task += gridDim.x) {
         const int n = (int)(task / nblk), b = (int)(task % nblk);
         const int p0 = b * GPB, np = min(GPB, M / 2 - p0);     // column pairs 2p, 2p+1
-        const real *fx = X + (size_t)n * M * M;
+        cx *fx = reinterpret_cast<cx *>(X + (size_t)n * M * M);  // row i, pair p at fx[i M/2 + p]
         __syncthreads();
         for (int e = threadIdx.x; e < M * np; e += blockDim.x) {
             const int i = e / np, p = e - i * np;
-            blue_cp(Z + (size_t)p * S + i, reinterpret_cast<const cx *>(fx + (size_t)i * M + 2 * (p0 + p)));
+            blue_cp(Z + (size_t)p * S + i, fx + (size_t)i * (M / 2) + p0 + p);
         }
         blue_cp_wait();
         __syncthreads();
@@ -523,33 +524,26 @@ kbl_colsE(const real *__restrict__ X, real *__restrict__ rho, const real *__rest
             }
         }
         __syncthreads();
-        const int bi = xc[n] - z + 1, bj = yc[n] - z + 1;
-        real *rcell = rho + (size_t)n * N * N;
-        const real *rb = Rb + (size_t)n * M * M, *dy = X + (size_t)Ntot * M * M + (size_t)n * M * M;
-        const int ncols = 2 * np;
-        constexpr int U = 4;              // four sites' loads in flight per thread
-        for (int e0 = threadIdx.x; e0 < M * ncols; e0 += U * blockDim.x) {
-            real ro[U], rr[U], yy[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const int e = e0 + u * blockDim.x;
-                if (e < M * ncols) {
-                    const int i = e / ncols, cc = e - i * ncols, col = 2 * p0 + cc;
-                    const size_t bo = (size_t)i * M + col;
-                    ro[u] = rcell[(size_t)(bi + i) * N + bj + col];
-                    rr[u] = rb[bo];
-                    yy[u] = dy[bo];
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const int e = e0 + u * blockDim.x;
-                if (e < M * ncols) {
-                    const int i = e / ncols, cc = e - i * ncols, col = 2 * p0 + cc;
-                    const cx w = Z[(size_t)(cc >> 1) * S + i];
-                    rcell[(size_t)(bi + i) * N + bj + col] = ro[u] + dtr * rr[u] + ((cc & 1 ? w.y : w.x) + yy[u]);
-                }
-            }
+        for (int e = threadIdx.x; e < M * np; e += blockDim.x) {
+            const int i = e / np, p = e - i * np;
+            fx[(size_t)i * (M / 2) + p0 + p] = Z[(size_t)p * S + i];
         }
+    }
+}
+
+// The new rho on every box: rho + (dt R + row term) + column term
+// (update_fft_rho and copy_to_rhon, rho_functions.cpp:213-265, by linearity;
+// planes 1 and 0 of X)
+template <typename real>
+__global__ void kbl_rho(const real *__restrict__ X, real *__restrict__ rho, const int *__restrict__ xc,
+                        const int *__restrict__ yc, int N, int z, int M, int Ntot) {
+    const int n = blockIdx.y;
+    const int bi = xc[n] - z + 1, bj = yc[n] - z + 1;
+    const real *dxc = X + (size_t)n * M * M, *q = X + (size_t)Ntot * M * M + (size_t)n * M * M;
+    real *rc = rho + (size_t)n * N * N;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < M * M; e += gridDim.x * blockDim.x) {
+        const int i = e / M, j = e - i * M;
+        real &ro = rc[(size_t)(bi + i) * N + bj + j];
+        ro = ro + (q[e] + dxc[e]);
     }
 }

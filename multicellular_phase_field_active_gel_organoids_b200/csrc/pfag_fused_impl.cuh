@@ -2732,17 +2732,19 @@ struct Fused {
             const long tasks = (long)Nt * (M / 2);
             pfag_prof_begin(c, "kbl_rowsD");
             kbl_rowsD<real, L><<<(unsigned)((tasks + BGm::GPB - 1) / BGm::GPB), BGm::THREADS, sm_rowsD, s>>>(
-                Y1, X, R(c->rho), c->d_xc, c->d_yc, N, z, M, Nt, tb, c->debug ? R(c->d_vx) : nullptr,
-                c->debug ? R(c->d_vy) : nullptr);
+                Y1, X, R(c->rho), R(r->Rb), c->dp.dt, c->d_xc, c->d_yc, N, z, M, Nt, tb,
+                c->debug ? R(c->d_vx) : nullptr, c->debug ? R(c->d_vy) : nullptr);
             PFAG_LAUNCHED(c);
         }
         {
             const long tasks = (long)Nt * ((M / 2 + BGm::GPB - 1) / BGm::GPB);
             pfag_prof_begin(c, "kbl_colsE");
-            kbl_colsE<real, L><<<(unsigned)tasks, BGm::THREADS, sm_colsE, s>>>(X, R(c->rho), R(r->Rb), c->d_xc,
-                                                                              c->d_yc, N, z, M, Nt, c->dp.dt, tb);
+            kbl_colsE<real, L><<<(unsigned)tasks, BGm::THREADS, sm_colsE, s>>>(X, M, Nt, tb);
             PFAG_LAUNCHED(c);
         }
+        pfag_prof_begin(c, "kbl_rho");
+        kbl_rho<real><<<g, 256, 0, s>>>(X, R(c->rho), c->d_xc, c->d_yc, N, z, M, Nt);
+        PFAG_LAUNCHED(c);
         return PFAG_OK;
     }
 
