@@ -160,12 +160,14 @@ def measured_peak_hbm():
 # committed ncu captures (dram__bytes_read.sum + dram__bytes_write.sum, one cold
 # launch) of the fused FP32 step: (config, kernel) -> (bytes, profile file).
 NCU_TRAFFIC = {
-    ("cfg1", "kr_boxB"): (58.4e6, "profiles/fused_cfg1_f32_top_kernels.md"),
-    ("cfg1", "kr_boxA"): (105.0e6, "profiles/fused_cfg1_f32_top_kernels.md"),
+    ("cfg1", "kr_boxA"): (96.5e6, "profiles/fused_cfg1_f32_top_kernels.md"),
+    ("cfg1", "kr_boxB"): (58.0e6, "profiles/fused_cfg1_f32_top_kernels.md"),
     ("cfg1", "kf_update_rows"): (77.8e6, "profiles/fused_cfg1_f32_top_kernels.md"),
+    ("cfg1", "kr_boxC2"): (55.9e6, "profiles/fused_cfg1_f32_top_kernels.md"),
     ("cfg1", "kr_boxD2"): (70.1e6, "profiles/fused_cfg1_f32_top_kernels.md"),
-    ("cfg1", "kr_boxC2"): (56.0e6, "profiles/fused_cfg1_f32_top_kernels.md"),
-    ("cfg1", "kf_resh_first"): (59.6e6, "profiles/fused_cfg1_f32_top_kernels.md"),
+    ("cfg1", "kf_resh_first"): (59.2e6, "profiles/fused_cfg1_f32_top_kernels.md"),
+    ("cfg1", "kf_hpsi"): (28.2e6, "profiles/fused_cfg1_f32_top_kernels.md"),
+    ("cfg1", "kf_relax_loops"): (19.2e6, "profiles/fused_cfg1_f32_top_kernels.md"),
 }
 
 

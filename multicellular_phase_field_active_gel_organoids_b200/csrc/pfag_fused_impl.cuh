@@ -1,6 +1,8 @@
 // Fused path: the same step as the plain path (and the reference loop body,
 // main_code/run_with_active_gels.cpp:123-182), restricted to the sites that
-// can change and fused into 13 launches per step with no host round trip.
+// can change, with no host round trip: about 18 kernels per step (9 on the
+// main stream, 9 on a side stream for the lumen/ECM work), replayed as one
+// CUDA graph from the second step on.
 //
 // Exactness of the restriction.  Every per-cell write of the reference step
 // lands in that cell's zone [xc-z, xc+z)^2, and hfunc_cell starts at zero, so
@@ -13,17 +15,21 @@
 // (norm_grad_phi, J_x/J_y, prod_norm_delta, temp_phase, the parameter maps,
 // pi_*) are recomputed on the fly where they are read.
 //
-// Spectral solve (rho_functions.cpp:409-471) per cell on the M x M box with
-// hand-written shared-memory FFTs in five passes:
-//   A rows:    stress pi_xx + i pi_yy and pi_xy, row FFT; reaction R stored
-//   B columns: column FFT, unpack, velocity (rho_functions.cpp:133-190),
-//              Hermitian projection packing Re(v_x) + i Re(v_y), column IFFT
-//   C rows:    row IFFT -> v; rho v / M^2 packed; row FFT
-//   D columns: column FFT, unpack, divergence term of update_fft_rho
-//              (rho_functions.cpp:230-249), Hermitian projection, column IFFT
-//   E rows:    row IFFT; rho_new = rho + dt R + Re(.)/M^2
-// By linearity of the transform this equals Re(IFFT(FFT(rho) + dt FFT(R) + D))/M^2
-// of the reference, without the two round-trip transforms of rho and R.
+// Spectral solve (rho_functions.cpp:409-471) per cell on its M x M box:
+//   M = 32..256 (power of two): four passes on register-resident FFTs
+//     A rows:    stresses pi_xx + i pi_yy and pi_xy, reaction R, class map, row FFTs
+//     B columns: column FFTs, the k-space velocity (rho_functions.cpp:133-190),
+//                Hermitian projection packing Re(v_x) + i Re(v_y), column IFFT
+//     C2 rows:   row IFFT -> v; Fx = rho vx stored; Fy = rho vy differentiated
+//                along the row (the separable form of update_fft_rho's divergence)
+//     D2 columns: Fx differentiated along the column; rho + dt R + both terms in place
+//   M = 16, 512, 1024: the same steps as five shared-memory radix-4 passes (kf_boxA..E)
+//   any other even M up to 512 (the reference's default zone_size 200 gives
+//     M = 398): Bluestein transforms over the register FFTs (pfag_bluestein.cuh;
+//     kg_stress, kbl_rowsA, kbl_colsB, kg_velocity, kbl_colsC, kbl_rowsD,
+//     kbl_colsE, kbl_rho).
+// By linearity of the transform the new rho equals Re(IFFT(FFT(rho) + dt FFT(R)
+// + D))/M^2 of the reference, without the round-trip transforms of rho and R.
 #pragma once
 #include "pfag_internal.cuh"
 #include "pfag_fft.cuh"

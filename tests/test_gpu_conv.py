@@ -39,7 +39,8 @@ def run_fwd(x, w, b, gelu_on, B, H, W, cin, cout):
 
 
 @pytest.mark.parametrize("B,H,W,cin,cout,gelu_on", [(2, 12, 20, 16, 32, True), (1, 128, 128, 32, 32, True),
-                                                  (3, 7, 9, 32, 16, False), (2, 33, 70, 16, 16, True)])
+                                                  (3, 7, 9, 32, 16, False), (2, 33, 70, 16, 16, True),
+                                                  (16, 128, 128, 32, 32, True)])
 def test_forward_matches_oracle(B, H, W, cin, cout, gelu_on):
     rng = np.random.default_rng(B * 1000 + H)
     x = co.pad(co.bf16(rng.normal(size=(B, H, W, cin))))
@@ -71,7 +72,8 @@ def test_input_gradient_through_flipped_weights():
     assert np.max(np.abs(dx[:, 1:-1, 1:-1, :] - ref)) <= 1e-2 * np.abs(ref).max()
 
 
-@pytest.mark.parametrize("B,H,W,cin,cout", [(2, 9, 13, 16, 32), (1, 128, 128, 32, 32), (3, 20, 31, 32, 16)])
+@pytest.mark.parametrize("B,H,W,cin,cout", [(2, 9, 13, 16, 32), (1, 128, 128, 32, 32), (3, 20, 31, 32, 16),
+                                            (16, 128, 128, 32, 32)])
 def test_weight_gradient_matches_oracle(B, H, W, cin, cout):
     rng = np.random.default_rng(H * 31 + W)
     x = co.pad(co.bf16(rng.normal(size=(B, H, W, cin))))
