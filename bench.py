@@ -11,6 +11,7 @@ step is timed with CUDA events on the context's stream.
 
   python bench.py --gpus N --steps K --warmup W            # this framework
   python bench.py --impl reference --steps K --warmup W    # reference on the host cores
+  python bench.py --gpus N --shard                         # one organoid's cells split over the N GPUs
 """
 from __future__ import annotations
 
@@ -47,6 +48,8 @@ def parse():
     ap.add_argument("--members", type=int, default=256, help="cfg3: organoids in the batched sweep")
     ap.add_argument("--no-tune", action="store_true", help="cfg3: default launch shapes (no autotuning)")
     ap.add_argument("--pairs", type=int, default=32, help="cfg4: coarse/fine training pairs")
+    ap.add_argument("--shard", action="store_true",
+                    help="split one organoid's cells over the ranks (psi all-reduce, neighbour halo): strong scaling")
     return ap.parse_args()
 
 
@@ -606,6 +609,8 @@ def main():
         return main_batched(args, ws, rank, local)
     if args.config == "cfg4":
         return main_corrector(args, ws, rank, local)
+    if args.shard and args.impl == "ours":
+        return main_sharded(args, ws, rank, local)
     cfg = CONFIGS[args.config]()
     config = {"workload": f"{args.config}: {cfg.N}x{cfg.N} periodic grid, {cfg.ncells} cells R={cfg.radius:g} "
                           f"on a jittered hexagonal lattice, zone_size {cfg.zone_size} (FFT box {cfg.box}), "
@@ -659,6 +664,87 @@ def main():
             "relax_iters_last_step": res["stats"]}
     if "compare" in res:
         line["compare_vs_plain_f64"] = res["compare"]
+    print(json.dumps(line))
+    return 0
+
+
+def main_sharded(args, ws, rank, local):
+    """One organoid (cfg) with its cells split over the ranks by contiguous
+    ranges (sharded.DistShard over NCCL): per step a halo of two phi planes
+    with the neighbouring ranks and an all-reduce of psi.  Total work is fixed
+    as N grows (strong scaling); value = the organoid's site-updates / the
+    slowest rank's time.  Each step is timed with CUDA events on the context's
+    stream, the L2 flush between steps outside them."""
+    import datetime
+    import torch
+    import torch.distributed as td
+    from multicellular_phase_field_active_gel_organoids_b200 import capi, sharded
+    from multicellular_phase_field_active_gel_organoids_b200.params import CONFIGS
+    torch.cuda.set_device(local)
+    if ws == 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        if "MASTER_PORT" not in os.environ:
+            import socket
+            so = socket.socket()
+            so.bind(("127.0.0.1", 0))
+            os.environ["MASTER_PORT"] = str(so.getsockname()[1])
+            so.close()
+        os.environ.setdefault("RANK", "0")
+        os.environ.setdefault("WORLD_SIZE", "1")
+    td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    cfg = CONFIGS[args.config]()
+    prec = args.precision
+    dtype = np.float64 if prec == 64 else np.float32
+    sites = cfg.ncells * cfg.N * cfg.N
+    sh = sharded.DistShard(cfg.params(), cfg.initial_state(dtype), precision=prec)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    it = 0
+    for _ in range(max(args.warmup, 3)):
+        sh.step(it, 1)
+        it += 1
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    td.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches = 0
+    with torch.cuda.stream(sh.stream):
+        for k in range(args.steps):
+            flush.fill_(k & 0xff)
+            ev[k][0].record(sh.stream)
+            sharded.run_steps(sh.ex, sh, it, 1)
+            launches += sh.sim.launch_count()
+            ev[k][1].record(sh.stream)
+            it += 1
+    torch.cuda.synchronize()
+    td.barrier()
+    clocks = sampler.stop()
+    sh.sim.sync()
+    total = torch.tensor([sum(a.elapsed_time(b) for a, b in ev)], dtype=torch.float64, device="cuda")
+    td.all_reduce(total, op=td.ReduceOp.MAX)
+    nl = torch.tensor([launches], dtype=torch.float64, device="cuda")
+    td.all_reduce(nl, op=td.ReduceOp.SUM)
+    stats = sh.sim.stats()
+    sh.close()
+    td.destroy_process_group()
+    if rank != 0:
+        return 0
+    total_ms = float(total.item())
+    value = sites * args.steps / (total_ms * 1e-3)
+    plane = cfg.N * cfg.N * (8 if prec == 64 else 4)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32" if prec == 32 else "f64",
+            "data": "synthetic (seeded organoid inputs generated in-process; no dataset)",
+            "config": {"workload": f"{args.config}: {cfg.N}x{cfg.N} grid, {cfg.ncells} cells, zone_size "
+                                   f"{cfg.zone_size} (FFT box {cfg.box}), cells split over {ws} rank(s)",
+                       "grid": cfg.N, "cells": cfg.ncells, "zone_size": cfg.zone_size, "box": cfg.box,
+                       "l2": "flushed between timed steps (256 MiB write)", "path": "fused",
+                       "parallelism": f"cell shards x{ws}", "cells_per_rank": [b - a for a, b in sh.bounds]},
+            "exchange_bytes_per_step_per_rank": {"psi_allreduce": plane, "halo": 2 * plane} if ws > 1 else {},
+            "roofline": None, "cpu_baseline": None, "e2e": None,
+            "gpu_launches": int(nl.item()), "clocks": clocks, "relax_iters_last_step": stats}
     print(json.dumps(line))
     return 0
 

@@ -86,6 +86,8 @@ int pfag_step(pfag_ctx *ctx, int it0, int nsteps);
 /* The same, enqueued on the context's stream without a final synchronisation
  * (device-resident benchmarking); errors surface at the next synchronous call. */
 int pfag_step_async(pfag_ctx *ctx, int it0, int nsteps);
+/* Wait for the context's stream, report device-side errors, and refresh the
+ * host copies of the observables and (fused path) the reshaping statistics. */
 int pfag_sync(pfag_ctx *ctx);
 
 /* Observables of the last step: s (Ntot doubles, cell areas), xc, yc (Ntot ints). */
@@ -162,6 +164,34 @@ int pfag_batch_sync(pfag_batch *b);
 void *pfag_batch_stream(pfag_batch *b);       /* cudaStream_t the parent graph is launched on */
 long pfag_batch_launch_count(pfag_batch *b);  /* kernel launches of the last step call */
 int pfag_batch_destroy(pfag_batch *b);
+
+/* ---- Cell sharding: one organoid's cells split over contexts by contiguous
+ * ranges (one context per GPU, or several on one GPU).  Cells couple only
+ * through psi = sum_n h(phi_n) (useful_functions.cpp:305-322) and the index
+ * neighbours' phi in the class map (rho_functions.cpp:297-311, cyclic over
+ * the organoid); lum and ECM are updated redundantly by every shard from the
+ * full psi.  A shard is a fused-path context created with Ntot = its cell
+ * count and the organoid's N_current.
+ * pfag_shard_enable allocates the context's two neighbour planes (N_s^2
+ * values each, the context's precision) and returns their device pointers:
+ * *lo holds phi of the cell before local cell 0, *hi phi of the cell after
+ * local cell Ntot-1; the host writes them before each step (they start as
+ * the context's own cells Ntot-1 and 0, i.e. an unsharded organoid).
+ * pfag_step_head enqueues the step up to this context's partial psi (over
+ * its own cells, in cell order; pfag_device_field "psi"); the host then
+ * completes psi on every shard (the sum over shards, the same values on
+ * every shard) and pfag_step_tail enqueues the rest of the step.  Both are
+ * asynchronous on the context's stream and replay CUDA graphs from the
+ * second step on; pfag_sync afterwards refreshes the observables.  Fused
+ * path only (PFAG_E_UNSUPPORTED otherwise); a tail without its head, or a
+ * whole-step call between them, returns PFAG_E_ARG.
+ * pfag_sum_planes: out[i] = parts[0][i] + parts[1][i] + ... in that order
+ * (1 <= nparts <= 64; precision 32 or 64; out may be one of the parts), on
+ * `stream` (cudaStream_t); with one part it is a device copy. */
+int pfag_shard_enable(pfag_ctx *ctx, void **lo, void **hi);
+int pfag_step_head(pfag_ctx *ctx, int it);
+int pfag_step_tail(pfag_ctx *ctx, int it);
+int pfag_sum_planes(void *out, const void *const *parts, int nparts, long count, int precision, void *stream);
 
 /* Per-kernel CUDA-event timing of the fused path on the context's stream.
  * pfag_profile_read synchronises and returns the number of kernels (<= cap):

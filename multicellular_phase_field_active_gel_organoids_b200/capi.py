@@ -67,6 +67,7 @@ EXPORTS = [
     "pfag_batch_stream", "pfag_batch_launch_count", "pfag_batch_destroy",
     "pfag_upload_device", "pfag_conv3x3", "pfag_conv3x3_wgrad", "pfag_conv_act_bwd", "pfag_conv_flip", "pfag_adam",
     "pfag_conv_mse", "pfag_corrector_gather", "pfag_corrector_apply",
+    "pfag_shard_enable", "pfag_step_head", "pfag_step_tail", "pfag_sum_planes", "pfag_device_field",
 ]
 
 
@@ -114,6 +115,10 @@ def lib() -> ctypes.CDLL:
         L.pfag_batch_launch_count.argtypes = [vp]
         L.pfag_batch_launch_count.restype = ctypes.c_long
         L.pfag_batch_destroy.argtypes = [vp]
+        L.pfag_shard_enable.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp)]
+        L.pfag_step_head.argtypes = [vp, ctypes.c_int]
+        L.pfag_step_tail.argtypes = [vp, ctypes.c_int]
+        L.pfag_sum_planes.argtypes = [vp, ctypes.POINTER(vp), ctypes.c_int, ctypes.c_long, ctypes.c_int, vp]
         i, f = ctypes.c_int, ctypes.c_float
         L.pfag_upload_device.argtypes = [vp, vp, vp, vp, vp]
         L.pfag_conv3x3.argtypes = [vp, vp, vp, vp, vp, i, i, i, i, i, i, vp, vp]
@@ -288,6 +293,20 @@ class Simulation:
     def stream(self) -> int:
         return int(lib().pfag_stream(self.h) or 0)
 
+    def shard_enable(self):
+        """(lo, hi) device pointers of the neighbour planes of a shard
+        (pfag_shard_enable): phi of the cells before local cell 0 and after
+        local cell ncells-1."""
+        lo, hi = ctypes.c_void_p(), ctypes.c_void_p()
+        check(lib().pfag_shard_enable(self.h, ctypes.byref(lo), ctypes.byref(hi)))
+        return int(lo.value), int(hi.value)
+
+    def step_head(self, it: int):
+        check(lib().pfag_step_head(self.h, int(it)))
+
+    def step_tail(self, it: int):
+        check(lib().pfag_step_tail(self.h, int(it)))
+
     def generate_initial(self, rho0: float, tol: float, make_fields: bool = True):
         """prepare_initial_files.cpp:53-117 on the device (plain-path context):
         the initial fields (make_fields) and their one-shot shaping."""
@@ -297,6 +316,14 @@ class Simulation:
         """Call one per-function entry point, e.g. fn("find_centres_cells")."""
         f = getattr(lib(), "pfag_fn_" + name)
         check(f(self.h, *args))
+
+
+def sum_planes(out: int, parts, count: int, precision: int, stream: int = 0) -> None:
+    """out[i] = parts[0][i] + parts[1][i] + ... in order, on the device
+    (pfag_sum_planes; device pointers as ints)."""
+    arr = (ctypes.c_void_p * len(parts))(*[int(p) for p in parts])
+    check(lib().pfag_sum_planes(ctypes.c_void_p(int(out)), arr, len(parts), int(count), int(precision),
+                                ctypes.c_void_p(int(stream))))
 
 
 class Batch:

@@ -261,6 +261,7 @@ extern "C" int pfag_sync(pfag_ctx *c) {
     if (!c) return PFAG_E_ARG;
     PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
     PFAG_TRY(pfag_check_device_error(c));
+    if (c->path == PFAG_PATH_FUSED && c->fused) PFAG_TRY(pfag_fused_stats(c));
     return pfag_fetch_observables(c);
 }
 

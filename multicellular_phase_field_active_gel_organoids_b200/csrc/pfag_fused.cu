@@ -13,6 +13,12 @@ int pfag_fused_stats_f64(pfag_ctx *c);
 int pfag_fused_stats_f32(pfag_ctx *c);
 int pfag_fused_recentre_f64(pfag_ctx *c);
 int pfag_fused_recentre_f32(pfag_ctx *c);
+int pfag_fused_step_part_f64(pfag_ctx *c, int part, bool sync_host);
+int pfag_fused_step_part_f32(pfag_ctx *c, int part, bool sync_host);
+
+int pfag_fused_stats(pfag_ctx *c) {
+    return c->prec == 64 ? pfag_fused_stats_f64(c) : pfag_fused_stats_f32(c);
+}
 
 int pfag_fused_recentre(pfag_ctx *c) {
     return c->prec == 64 ? pfag_fused_recentre_f64(c) : pfag_fused_recentre_f32(c);
@@ -33,7 +39,7 @@ void pfag_fused_free(pfag_ctx *c) {
     for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);
     void *bufs[] = {r->Y1, r->Y2, r->Rb, r->clsT, r->Jc, r->Jl, r->rect, r->part_r, r->part_e, r->part_l,
                     r->part_lt, r->part_a, r->cK, r->G, r->Gsp, r->btw, r->bcw, r->bwf,
-                    r->bhdi, r->bh};
+                    r->bhdi, r->bh, r->nb_lo};
     for (void *b : bufs) if (b) cudaFree(b);
     delete r;
     c->fused = nullptr;
@@ -196,3 +202,73 @@ extern "C" int pfag_batch_step(pfag_batch *b, int it0, int nsteps) {
 
 extern "C" void *pfag_batch_stream(pfag_batch *b) { return b ? (void *)b->stream : nullptr; }
 extern "C" long pfag_batch_launch_count(pfag_batch *b) { return b ? b->launches : -1; }
+
+// ---- cell sharding: one organoid's cells split over contexts ------------------
+// (contiguous cell ranges; cells couple through psi and the index neighbours'
+// phi, rho_functions.cpp:297-311, useful_functions.cpp:305-322)
+extern "C" int pfag_shard_enable(pfag_ctx *c, void **lo, void **hi) {
+    if (!c || !lo || !hi) { pfag_set_error("null argument"); return PFAG_E_ARG; }
+    if (c->path != PFAG_PATH_FUSED) { pfag_set_error("cell sharding runs on the fused path"); return PFAG_E_UNSUPPORTED; }
+    FusedRes *r = F(c);
+    if (!r->nb_lo) {
+        const size_t plane = (size_t)c->N * c->N * (c->prec == 64 ? 8 : 4);
+        PFAG_CUDA_CHECK(cudaMalloc(&r->nb_lo, 2 * plane));
+        r->nb_hi = (char *)r->nb_lo + plane;
+        // until the host writes them: this context's own cyclic neighbours
+        PFAG_CUDA_CHECK(cudaMemcpyAsync(r->nb_lo, (const char *)c->phi + (size_t)(c->Ntot - 1) * plane, plane,
+                                        cudaMemcpyDeviceToDevice, c->stream));
+        PFAG_CUDA_CHECK(cudaMemcpyAsync(r->nb_hi, c->phi, plane, cudaMemcpyDeviceToDevice, c->stream));
+        PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+        fused_drop_graph(r);          // captured steps read the previous neighbour planes
+        r->graph_state = 0;
+    }
+    *lo = r->nb_lo;
+    *hi = r->nb_hi;
+    return PFAG_OK;
+}
+
+static int step_part(pfag_ctx *c, int part) {
+    if (!c) { pfag_set_error("null ctx"); return PFAG_E_ARG; }
+    if (c->path != PFAG_PATH_FUSED) { pfag_set_error("the split step runs on the fused path"); return PFAG_E_UNSUPPORTED; }
+    if (part == 1) c->launches = 0;
+    return c->prec == 64 ? pfag_fused_step_part_f64(c, part, false) : pfag_fused_step_part_f32(c, part, false);
+}
+extern "C" int pfag_step_head(pfag_ctx *c, int) { return step_part(c, 1); }
+extern "C" int pfag_step_tail(pfag_ctx *c, int) { return step_part(c, 2); }
+
+// out[i] = ((parts[0][i] + parts[1][i]) + parts[2][i]) + ...: the shards' psi
+// partials in shard order (out may be one of the parts)
+constexpr int SUM_MAX_PARTS = 64;
+template <typename real> struct PartList { const real *p[SUM_MAX_PARTS]; };
+template <typename real>
+__global__ void k_sum_planes(real *out, PartList<real> L, int nparts, long count) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (long)gridDim.x * blockDim.x) {
+        real v = L.p[0][i];
+        for (int k = 1; k < nparts; k++) v += L.p[k][i];
+        out[i] = v;
+    }
+}
+
+template <typename real>
+static int sum_planes_t(void *out, const void *const *parts, int nparts, long count, cudaStream_t s) {
+    PartList<real> L{};
+    for (int k = 0; k < nparts; k++) L.p[k] = (const real *)parts[k];
+    const long blocks = std::min<long>((count + 255) / 256, 148L * 8);
+    k_sum_planes<real><<<(unsigned)std::max(1L, blocks), 256, 0, s>>>((real *)out, L, nparts, count);
+    PFAG_CUDA_CHECK(cudaGetLastError());
+    return PFAG_OK;
+}
+
+extern "C" int pfag_sum_planes(void *out, const void *const *parts, int nparts, long count, int precision,
+                               void *stream) {
+    if (!out || !parts || nparts < 1 || nparts > SUM_MAX_PARTS || count < 0 || (precision != 32 && precision != 64)) {
+        pfag_set_error("pfag_sum_planes: bad arguments");
+        return PFAG_E_ARG;
+    }
+    for (int k = 0; k < nparts; k++)
+        if (!parts[k]) { pfag_set_error("pfag_sum_planes: null part"); return PFAG_E_ARG; }
+    if (count == 0) return PFAG_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    return precision == 64 ? sum_planes_t<double>(out, parts, nparts, count, s)
+                           : sum_planes_t<float>(out, parts, nparts, count, s);
+}

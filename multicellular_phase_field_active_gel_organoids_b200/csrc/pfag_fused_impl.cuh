@@ -105,6 +105,18 @@ struct FusedRes {
     int logm, rows_blk, grp_cols;
     size_t smemA, smemB, smemC, smemD, smemE;
     bool ring_pending;      // the rho ghost ring still has to be made to match its sources
+    // cell sharding (pfag_shard_enable): [2][N][N] phi planes of the cells
+    // before local cell 0 and after local cell Ntot-1, held by other contexts
+    // and written here by the host between steps; null when unsharded
+    void *nb_lo, *nb_hi;
+    // the step split at psi (pfag_step_head / pfag_step_tail), each part
+    // captured as its own graph: [0] head, [1] tail
+    cudaGraph_t pgraph[2];
+    cudaGraphExec_t pgexec[2];
+    bool pgraph_ok[2];
+    int pgraph_state[2];
+    long pgraph_launches[2];
+    bool head_pending;      // a head was enqueued and its tail not yet
     // one step captured as a CUDA graph after the first eager step
     cudaGraph_t graph;
     cudaGraphExec_t gexec;
@@ -455,7 +467,20 @@ struct BoxArgs {
     double c4, sigma, dt, kfac, friction, dx;
     double inv_2s2, k_delta;     // 1/(2 sigma^2), 1/(sqrt(2 pi) sigma): FP32 folded constants
     double deg[3], gen[3], a_ort[3], a_tan[3], visc[3], bb[3];
+    // phi planes of the index neighbours of cells 0 and Ntot-1 (n1 of cell 0
+    // and n2 of cell Ntot-1, rho_functions.cpp:297-311): this context's own
+    // cells Ntot-1 and 0, or planes held for a shard of a larger organoid
+    const void *nb_lo, *nb_hi;
 };
+
+// the phi planes of cell n's index neighbours n1 = n-1 and n2 = n+1 (cyclic over the organoid)
+template <typename real>
+__device__ __forceinline__ void nb_planes(const real *phi, const BoxArgs &a, int n, const real *&p1,
+                                          const real *&p2) {
+    const size_t NN = (size_t)a.N * a.N;
+    p1 = (n == 0) ? (const real *)a.nb_lo : phi + (size_t)(n - 1) * NN;
+    p2 = (n == a.Ntot - 1) ? (const real *)a.nb_hi : phi + (size_t)(n + 1) * NN;
+}
 
 __device__ __forceinline__ int wrapk(int i, int M) { return i < M / 2 ? i : i - M; }
 
@@ -474,8 +499,8 @@ __global__ void kf_boxA(const real *__restrict__ phi, const real *__restrict__ r
     fft_twiddles(tw, M);
     const int n = blockIdx.y, i0 = blockIdx.x * R;
     const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
-    const int n1 = (n == 0) ? a.Ntot - 1 : n - 1;
-    const int n2 = (n == a.Ntot - 1) ? 0 : n + 1;
+    const real *p1, *p2;
+    nb_planes<real>(phi, a, n, p1, p2);
     const size_t NN = (size_t)N * N;
     const real *p = phi + (size_t)n * NN;
     const real c4 = (real)a.c4, sigma = (real)a.sigma;
@@ -488,7 +513,7 @@ __global__ void kf_boxA(const real *__restrict__ phi, const real *__restrict__ r
         const real dxp = p[s + N] - p[s - N];
         const real dyp = p[s + 1] - p[s - 1];
         const real g = sqrt(c4 * (dxp * dxp + dyp * dyp));
-        const int cls = map_class_f<real>(f, lum[s], ecm[s], phi[(size_t)n1 * NN + s], phi[(size_t)n2 * NN + s]);
+        const int cls = map_class_f<real>(f, lum[s], ecm[s], p1[s], p2[s]);
         const real rr = rho[(size_t)n * NN + s];
         const real at = (real)a.a_tan[cls], ao = (real)a.a_ort[cls], b = (real)a.bb[cls];
         // compute_pi_xx/yy/xy, rho_functions.cpp:47-51, :75-79, :105-109
@@ -851,8 +876,8 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) kr_boxA(const 
     const int n = blockIdx.y, i0 = blockIdx.x * ROWS, i = i0 + g;
     const int N = a.N;
     const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
-    const int n1 = (n == 0) ? a.Ntot - 1 : n - 1;
-    const int n2 = (n == a.Ntot - 1) ? 0 : n + 1;
+    const real *p1, *p2;
+    nb_planes<real>(phi, a, n, p1, p2);
     const size_t NN = (size_t)N * N;
     const real *p = phi + (size_t)n * NN;
     // the block's phi rows with a one-site halo ([ROWS + 2][M + 2], in the FFT
@@ -889,8 +914,7 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) kr_boxA(const 
         const real dyp = sphi[o + 1] - sphi[o - 1];
         real xx, yy, xy, rt;
         int c;
-        box_stress<real>(a, f, dxp, dyp, xys[g * M + j], lum[s], ecm[s], phi[(size_t)n1 * NN + s],
-                         phi[(size_t)n2 * NN + s], xx, yy, xy, rt, c);
+        box_stress<real>(a, f, dxp, dyp, xys[g * M + j], lum[s], ecm[s], p1[s], p2[s], xx, yy, xy, rt, c);
         Rb[rowo + j] = rt;
         cls[g * (M + 4) + j] = (unsigned char)c;
         xys[g * M + j] = xy;
@@ -1260,13 +1284,14 @@ __global__ void kg_stress(const real *__restrict__ phi, const real *__restrict__
     if (e >= M * M) return;
     const int i = e / M, j = e - i * M;
     const int bi = xc[n] - a.z + 1, bj = yc[n] - a.z + 1;
-    const int n1 = (n == 0) ? a.Ntot - 1 : n - 1, n2 = (n == a.Ntot - 1) ? 0 : n + 1;
+    const real *p1, *p2;
+    nb_planes<real>(phi, a, n, p1, p2);
     const size_t NN = (size_t)N * N, s = (size_t)(bi + i) * N + (bj + j);
     const real *p = phi + (size_t)n * NN;
     real xx, yy, xy, rt;
     int c;
     box_stress<real>(a, p[s], p[s + N] - p[s - N], p[s + 1] - p[s - 1], rho[(size_t)n * NN + s], lum[s], ecm[s],
-                     phi[(size_t)n1 * NN + s], phi[(size_t)n2 * NN + s], xx, yy, xy, rt, c);
+                     p1[s], p2[s], xx, yy, xy, rt, c);
     const size_t o = (size_t)n * M * M + e;
     Y1[o].x = xx;
     Y1[o].y = yy;
@@ -2273,6 +2298,10 @@ BoxArgs box_args(pfag_ctx *c) {
         a.deg[k] = d.deg[k]; a.gen[k] = d.gen[k]; a.a_ort[k] = d.a_ort[k]; a.a_tan[k] = d.a_tan[k];
         a.visc[k] = d.visc[k]; a.bb[k] = d.bb[k];
     }
+    const FusedRes *r = F(c);
+    const size_t plane = (size_t)c->N * c->N * (c->prec == 64 ? 8 : 4);
+    a.nb_lo = r->nb_lo ? r->nb_lo : (const void *)((const char *)c->phi + (size_t)(c->Ntot - 1) * plane);
+    a.nb_hi = r->nb_hi ? r->nb_hi : (const void *)c->phi;
     return a;
 }
 
@@ -2505,8 +2534,10 @@ struct Fused {
         return PFAG_OK;
     }
 
-    // enqueue one step (no host synchronisation; capturable)
-    int enqueue() {
+    // enqueue one step (no host synchronisation; capturable).  part 0: the
+    // whole step; 1: its head (centroids, h, this context's psi); 2: the rest,
+    // once the host has completed psi over every shard of the organoid
+    int enqueue(int part = 0) {
         cudaStream_t s = c->stream;
         const int N = c->N, Nt = c->Ntot, M = c->M, z = c->zone;
         const DevParams &d = c->dp;
@@ -2514,12 +2545,18 @@ struct Fused {
         //    or the upload, left over B_n), hfunc on the zones, psi, area
         //    partials, h(lum), h(ECM), sum_ecm partials
         const int tiles = (N + 31) / 32, tiles_r = (N + PT_R - 1) / PT_R;
-        pfag_prof_begin(c, "kf_hpsi");
-        kf_hpsi<real><<<dim3(tiles, tiles_r), FT, 0, s>>>(R(c->phi), R(c->hfunc), r->rect, c->d_cacc, c->d_xc,
-                                                           c->d_yc, c->d_err, Nt, N, z,
-                                                         R(c->lum), R(c->ecm), R(c->psi), R(c->hlum), R(c->hecm),
-                                                         d.dx * d.dx, r->part_e, r->part_a);
-        PFAG_LAUNCHED(c);
+        if (part != 2) {
+            pfag_prof_begin(c, "kf_hpsi");
+            kf_hpsi<real><<<dim3(tiles, tiles_r), FT, 0, s>>>(R(c->phi), R(c->hfunc), r->rect, c->d_cacc, c->d_xc,
+                                                               c->d_yc, c->d_err, Nt, N, z, R(c->lum), R(c->ecm),
+                                                               R(c->psi), R(c->hlum), R(c->hecm), d.dx * d.dx,
+                                                               r->part_e, r->part_a);
+            PFAG_LAUNCHED(c);
+            if (part == 1) {
+                PFAG_CUDA_CHECK(cudaGetLastError());
+                return PFAG_OK;
+            }
+        }
         // 3. areas and f0, then the lumen / ECM update and normals
         //    (cell_phase_functions.cpp:372-444, :722-771), which need only psi,
         //    h(lum) and h(ECM): on the side stream beside pass A, the phi
@@ -2852,6 +2889,66 @@ template <typename real> int fused_upload_t(pfag_ctx *c) { return Fused<real>(c)
 inline void fused_drop_graph(FusedRes *r) {
     if (r->graph_ok) { cudaGraphExecDestroy(r->gexec); cudaGraphDestroy(r->graph); }
     r->graph_ok = false;
+    for (int k = 0; k < 2; k++) {
+        if (r->pgraph_ok[k]) { cudaGraphExecDestroy(r->pgexec[k]); cudaGraphDestroy(r->pgraph[k]); }
+        r->pgraph_ok[k] = false;
+        r->pgraph_state[k] = 0;
+    }
+}
+
+// One part of a step split at psi (part 1: head, 2: tail), graph-captured
+// like the whole step once an eager step has run: the head after the first
+// eager head-and-tail, the tail likewise.
+template <typename real> int fused_step_part_t(pfag_ctx *c, int part, bool sync_host) {
+    FusedRes *r = F(c);
+    if ((part == 1) == r->head_pending) {
+        pfag_set_error(part == 1 ? "step head enqueued twice without its tail" : "step tail without its head");
+        return PFAG_E_ARG;
+    }
+    const int k = part - 1;
+    const bool graphable = !pfag_prof_on(c) && !c->debug && !std::getenv("PFAG_NO_GRAPH");
+    if (r->graph_key != (long)c->relax_cap) {
+        fused_drop_graph(r);
+        r->graph_state = 0;
+        r->graph_key = (long)c->relax_cap;
+    }
+    if (graphable && r->pgraph_state[k] == 0 && r->eager_steps >= 1 && !r->ring_pending) {
+        cudaStream_t s = c->stream;
+        const long l0 = c->launches;
+        r->pgraph_state[k] = -1;
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const int rc = Fused<real>(c).enqueue(part);
+            cudaGraph_t g = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(s, &g);
+            if (rc == PFAG_OK && e == cudaSuccess && g && cudaGraphInstantiate(&r->pgexec[k], g, 0) == cudaSuccess) {
+                r->pgraph[k] = g;
+                r->pgraph_ok[k] = true;
+                r->pgraph_state[k] = 1;
+                r->pgraph_launches[k] = c->launches - l0;
+            } else if (g) {
+                cudaGraphDestroy(g);
+            }
+        }
+        c->launches = l0;
+        (void)cudaGetLastError();
+    }
+    if (r->pgraph_ok[k] && !r->ring_pending && graphable) {
+        PFAG_CUDA_CHECK(cudaGraphLaunch(r->pgexec[k], c->stream));
+        c->launches += r->pgraph_launches[k];
+    } else {
+        const int rc = Fused<real>(c).enqueue(part);
+        if (rc != PFAG_OK) return rc;
+        if (part == 2) {
+            r->eager_steps++;
+            r->ring_pending = false;
+        }
+    }
+    r->head_pending = part == 1;
+    if (sync_host && part == 2) {
+        PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+        return Fused<real>(c).stats();
+    }
+    return PFAG_OK;
 }
 
 // One step.  The first step runs eagerly (kernel attributes and the
@@ -2861,6 +2958,7 @@ inline void fused_drop_graph(FusedRes *r) {
 // back to it for good.
 template <typename real> int fused_step_t(pfag_ctx *c, bool sync_host) {
     FusedRes *r = F(c);
+    if (r->head_pending) { pfag_set_error("a step head is waiting for its tail"); return PFAG_E_ARG; }
     const bool graphable = !pfag_prof_on(c) && !c->debug && !std::getenv("PFAG_NO_GRAPH");
     const long key = (long)c->relax_cap;
     if (r->graph_ok && r->graph_key != key) {

@@ -135,6 +135,7 @@ int pfag_fused_step(pfag_ctx *ctx, int it, bool sync_host);
 int pfag_check_device_error(pfag_ctx *ctx);
 int pfag_after_upload(pfag_ctx *ctx);
 int pfag_fused_recentre(pfag_ctx *ctx);
+int pfag_fused_stats(pfag_ctx *c);        // reshaping iteration counts of the last step into c->stats
 int pfag_fetch_observables(pfag_ctx *ctx);
 
 // ---------------------------------------------------------------------------

@@ -7,8 +7,9 @@ one batch job per folder (:119-127).  Here the same expansion gives the same
 members in the same order, each member's parameter set is the one its
 constants.cpp would hold (written as a key/value file into the member's
 folder), and all members advance together on one GPU: one context (device
-state and CUDA graph) per member, each on its own stream, so small organoids
-that do not fill the GPU alone run side by side.  Every member starts from the
+state and CUDA graph) per member and, on the fused path, one graph launch per
+step over every member (capi.Batch, the batched engine of batched.py), so small
+organoids that do not fill the GPU alone run side by side.  Every member starts from the
 same initial state files, as the reference copies the same ini_*.bin files
 into every folder (:101-103); a member with N_ini cells reads the first N_ini.
 """
@@ -89,6 +90,7 @@ class Sweep:
         """`initial` = (phi, rho, lum, ECM) with at least max(N_ini) cells."""
         self.params = [member_params(m, base) for m in members]
         self.sims = []
+        self.batch = None
         phi, rho, lum, ecm = initial
         dtype = np.float64 if precision == 64 else np.float32
         try:
@@ -99,15 +101,25 @@ class Sweep:
                 n = int(p["N_ini"])
                 s.upload(*(np.ascontiguousarray(a, dtype=dtype) for a in (phi[:n], rho[:n], lum, ecm)))
                 self.sims.append(s)
+            if path == capi.PATH_FUSED:
+                self.batch = capi.Batch(self.sims)
         except Exception:
             self.close()
             raise
 
-    def step(self, it0: int, nsteps: int = 1) -> None:
-        """nsteps steps of every member; members' launches interleave step by step."""
-        for k in range(nsteps):
+    def _step_async(self, it: int) -> None:
+        if self.batch is not None:
+            self.batch.step_async(it, 1)      # one graph launch over every member
+        else:
             for s in self.sims:
-                s.step_async(it0 + k, 1)
+                s.step_async(it, 1)
+
+    def step(self, it0: int, nsteps: int = 1) -> None:
+        """nsteps steps of every member."""
+        for k in range(nsteps):
+            self._step_async(it0 + k)
+        if self.batch is not None:
+            self.batch.sync()
         for s in self.sims:
             s.sync()
 
@@ -123,10 +135,12 @@ class Sweep:
                 P.write_param_file(p, os.path.join(d, "constants.txt"))
                 writers.append(SnapshotWriter(s, d, text=text, slots=2))
             for it in range(nsteps):
-                for w, s in zip(writers, self.sims):
-                    if it % nsaving == 0:
+                if it % nsaving == 0:
+                    for w in writers:
                         w.save(it)
-                    s.step_async(it, 1)
+                self._step_async(it)
+            if self.batch is not None:
+                self.batch.sync()
             for s in self.sims:
                 s.sync()
         finally:
@@ -138,6 +152,9 @@ class Sweep:
         return [s.download() for s in self.sims]
 
     def close(self):
+        if self.batch is not None:
+            self.batch.close()
+            self.batch = None
         for s in self.sims:
             s.close()
         self.sims = []
