@@ -246,8 +246,10 @@ def kernel_bytes(cfg, precision: int, iters: dict, ubox: int, uring: int) -> dic
         "kg_velocity": box * (2 * w + w + 1 + 2 * w),
         # inverse columns: Y1 read and written
         "kbl_colsC": box * 4 * w,
-        # inverse rows: reads Y1, rho and R; writes Fx and dt R + the row term
-        "kbl_rowsD": box * (2 * w + w + w + 2 * w),
+        # inverse rows: reads Y1 and rho; writes Fx and Fy
+        "kbl_rowsD1": box * (2 * w + w + 2 * w),
+        # row derivative: reads Fy and R; writes dt R + the row term over Fy
+        "kbl_rowsD2": box * 3 * w,
         # column derivative: reads Fx, writes it differentiated
         "kbl_colsE": box * 2 * w,
         # the new rho: reads both terms and rho, writes rho

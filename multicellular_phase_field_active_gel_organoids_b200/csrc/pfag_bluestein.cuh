@@ -394,18 +394,19 @@ kbl_cols(ColSet<typename Cplx<real>::type> s0, ColSet<typename Cplx<real>::type>
     }
 }
 
-// Pass D' (rows, inverse): for rows i, i+1 of a cell, the inverse row
-// transforms of Y1 give M^2 (vx + i vy); Fx = rho vx / M^2 is stored in X
-// (plane 0, row-major) for the column pass, and Fy = rho vy / M^2 of the two
-// rows is differentiated along the row at once (one complex convolution);
-// plane 1 receives dt R + that row term (dt kfac folded in) (load_fft_rho_v
-// and the row half of update_fft_rho, rho_functions.cpp:213-284).
+// Pass D' (rows, inverse) in two kernels, so that each holds one transform's
+// state (184 and 68 bytes of spills at 128 registers, against 592 for both
+// transforms in one kernel): kbl_rowsD1 takes the inverse row transform of one
+// row of Y1 (M^2 (vx + i vy)) and stores Fx = rho vx / M^2 into plane 0 and
+// Fy = rho vy / M^2 into plane 1 of X (load_fft_rho_v, rho_functions.cpp:
+// 213-284); kbl_rowsD2 differentiates Fy along the row, two rows as one
+// complex sequence, and overwrites plane 1 with dt R + that row term (dt kfac
+// folded in; the row half of update_fft_rho).
 template <typename real, int L>
 __global__ void __launch_bounds__(BlueGeom<real, L>::THREADS, BlueGeom<real, L>::MINB)
-kbl_rowsD(const typename Cplx<real>::type *__restrict__ Y1, real *__restrict__ X, const real *__restrict__ rho,
-          const real *__restrict__ Rb, double dt, const int *__restrict__ xc, const int *__restrict__ yc, int N,
-          int z, int M, int Ntot, BlueTabs<typename Cplx<real>::type> tb, real *__restrict__ vdx,
-          real *__restrict__ vdy) {
+kbl_rowsD1(const typename Cplx<real>::type *__restrict__ Y1, real *__restrict__ X, const real *__restrict__ rho,
+           const int *__restrict__ xc, const int *__restrict__ yc, int N, int z, int M, int Ntot,
+           BlueTabs<typename Cplx<real>::type> tb, real *__restrict__ vdx, real *__restrict__ vdy) {
     typedef typename Cplx<real>::type cx;
     typedef Blue<cx, L> B;
     constexpr int TT = B::TT, E1 = B::E1, GPB = BlueGeom<real, L>::GPB;
@@ -413,59 +414,76 @@ kbl_rowsD(const typename Cplx<real>::type *__restrict__ Y1, real *__restrict__ X
     cx *tw = (cx *)smraw;
     const int t = threadIdx.x % TT, g = threadIdx.x / TT;
     cx *sm = tw + L + (size_t)g * L;
-    real *fys0 = reinterpret_cast<real *>(tw + L + (size_t)GPB * L);
-    real *fys = fys0 + (size_t)g * 2 * M;   // Fy of the two rows
     load_tw<cx, L>(tw, tb.tw);
     unsigned char *end;
-    const BlueTabs<cx> st = stage_tabs<cx, L>(tb, reinterpret_cast<unsigned char *>(fys0 + (size_t)GPB * 2 * M), M,
-                                              true, true, &end);
+    const BlueTabs<cx> st = stage_tabs<cx, L>(tb, reinterpret_cast<unsigned char *>(tw + L + (size_t)GPB * L), M,
+                                              true, false, &end);
     __syncthreads();
-    const int per = M / 2;
-    const long total = (long)Ntot * per;
+    const long total = (long)Ntot * M;
     const real mm = (real)((double)M * (double)M);
+    real *Fy = X + (size_t)Ntot * M * M;
     for (long base = (long)blockIdx.x * GPB; base < total; base += (long)gridDim.x * GPB) {
         const long task = base + g;
         const bool live = task < total;
-        const int n = live ? (int)(task / per) : 0, i0 = live ? 2 * (int)(task % per) : 0;
+        const int n = live ? (int)(task / M) : 0, i = live ? (int)(task % M) : 0;
         const int bi = xc[n] - z + 1, bj = yc[n] - z + 1;
-#pragma unroll 1
-        for (int h = 0; h < 2; h++) {
-            const int i = i0 + h;
-            const size_t rowo = ((size_t)n * M + i) * M;
-            cx v[E1];
+        const size_t rowo = ((size_t)n * M + i) * M;
+        cx v[E1];
 #pragma unroll
-            for (int q = 0; q < E1; q++) {
-                const int j = B::idx(t, q);
-                v[q] = (live && j < M) ? Y1[rowo + j] : CxOps<cx>::mk((real)0.0, (real)0.0);
-            }
-            B::template dft<true>(v, t, M, sm, tw, st);
+        for (int q = 0; q < E1; q++) {
+            const int j = B::idx(t, q);
+            v[q] = (live && j < M) ? Y1[rowo + j] : CxOps<cx>::mk((real)0.0, (real)0.0);
+        }
+        B::template dft<true>(v, t, M, sm, tw, st);
+        if (live) {
             const real *rh = rho + (size_t)n * N * N + (size_t)(bi + i) * N + bj;
 #pragma unroll
             for (int q = 0; q < E1; q++) {
                 const int j = B::idx(t, q);
                 if (j < M) {
-                    real f = (real)0.0;
-                    if (live) {
-                        const real rr = rh[j];
-                        X[rowo + j] = rr * v[q].x / mm;      // load_fft_rho_v, rho_functions.cpp:279
-                        f = rr * v[q].y / mm;
-                        if (vdx) { vdx[rowo + j] = v[q].x / mm; vdy[rowo + j] = v[q].y / mm; }
-                    }
-                    fys[h * M + j] = f;      // read back by the same thread
+                    const real rr = rh[j];
+                    X[rowo + j] = rr * v[q].x / mm;
+                    Fy[rowo + j] = rr * v[q].y / mm;
+                    if (vdx) { vdx[rowo + j] = v[q].x / mm; vdy[rowo + j] = v[q].y / mm; }
                 }
             }
         }
+    }
+}
+
+template <typename real, int L>
+__global__ void __launch_bounds__(BlueGeom<real, L>::THREADS, BlueGeom<real, L>::MINB)
+kbl_rowsD2(real *__restrict__ X, const real *__restrict__ Rb, double dt, int M, int Ntot,
+           BlueTabs<typename Cplx<real>::type> tb) {
+    typedef typename Cplx<real>::type cx;
+    typedef Blue<cx, L> B;
+    constexpr int TT = B::TT, E1 = B::E1, GPB = BlueGeom<real, L>::GPB;
+    extern __shared__ unsigned char smraw[];
+    cx *tw = (cx *)smraw;
+    const int t = threadIdx.x % TT, g = threadIdx.x / TT;
+    cx *sm = tw + L + (size_t)g * L;
+    load_tw<cx, L>(tw, tb.tw);
+    unsigned char *end;
+    const BlueTabs<cx> st = stage_tabs<cx, L>(tb, reinterpret_cast<unsigned char *>(tw + L + (size_t)GPB * L), M,
+                                              false, true, &end);
+    __syncthreads();
+    const int per = M / 2;
+    const long total = (long)Ntot * per;
+    const real dtr = (real)dt;
+    for (long base = (long)blockIdx.x * GPB; base < total; base += (long)gridDim.x * GPB) {
+        const long task = base + g;
+        const bool live = task < total;
+        const int n = live ? (int)(task / per) : 0, i0 = live ? 2 * (int)(task % per) : 0;
+        real *d0 = X + (size_t)Ntot * M * M + ((size_t)n * M + i0) * M;     // Fy rows i0, i0 + 1
         cx v[E1];
 #pragma unroll
         for (int q = 0; q < E1; q++) {
             const int j = B::idx(t, q);
-            v[q] = (j < M) ? CxOps<cx>::mk(fys[j], fys[M + j]) : CxOps<cx>::mk((real)0.0, (real)0.0);
+            v[q] = (live && j < M) ? CxOps<cx>::mk(d0[j], d0[M + j]) : CxOps<cx>::mk((real)0.0, (real)0.0);
         }
         B::deriv(v, t, M, sm, tw, st);
         if (live) {
-            real *d0 = X + (size_t)Ntot * M * M + ((size_t)n * M + i0) * M;
             const real *r0 = Rb + ((size_t)n * M + i0) * M;
-            const real dtr = (real)dt;
 #pragma unroll
             for (int q = 0; q < E1; q++) {
                 const int j = B::idx(t, q);

@@ -26,7 +26,7 @@
 //   M = 16, 512, 1024: the same steps as five shared-memory radix-4 passes (kf_boxA..E)
 //   any other even M up to 512 (the reference's default zone_size 200 gives
 //     M = 398): Bluestein transforms over the register FFTs (pfag_bluestein.cuh;
-//     kg_stress, kbl_rowsA, kbl_colsB, kg_velocity, kbl_colsC, kbl_rowsD,
+//     kg_stress, kbl_rowsA, kbl_colsB, kg_velocity, kbl_colsC, kbl_rowsD1/D2,
 //     kbl_colsE, kbl_rho).
 // By linearity of the transform the new rho equals Re(IFFT(FFT(rho) + dt FFT(R)
 // + D))/M^2 of the reference, without the round-trip transforms of rho and R.
@@ -2733,12 +2733,13 @@ struct Fused {
         const size_t cs = sizeof(cx);
         const size_t tab_c = tabs_bytes<cx, L>(M, true, false), tab_d = tabs_bytes<cx, L>(M, false, true);
         const size_t sm_rows = (size_t)(1 + BGm::GPB) * L * cs + tab_c;
-        const size_t sm_rowsD = (size_t)(1 + BGm::GPB) * L * cs + (size_t)BGm::GPB * 2 * M * sizeof(real) +
-                                tabs_bytes<cx, L>(M, true, true);
+        const size_t sm_rowsD1 = (size_t)(1 + BGm::GPB) * L * cs + tab_c;
+        const size_t sm_rowsD2 = (size_t)(1 + BGm::GPB) * L * cs + tab_d;
         const size_t sm_cols = ((size_t)L + (size_t)BGm::GPB * (L + 1)) * cs + tab_c;
         const size_t sm_colsE = ((size_t)L + (size_t)BGm::GPB * (L + 1)) * cs + tab_d;
         PFAG_TRY(smem_at_least((const void *)kbl_rowsA<real, L>, sm_rows));
-        PFAG_TRY(smem_at_least((const void *)kbl_rowsD<real, L>, sm_rowsD));
+        PFAG_TRY(smem_at_least((const void *)kbl_rowsD1<real, L>, sm_rowsD1));
+        PFAG_TRY(smem_at_least((const void *)kbl_rowsD2<real, L>, sm_rowsD2));
         PFAG_TRY(smem_at_least((const void *)kbl_cols<real, L, false>, sm_cols));
         PFAG_TRY(smem_at_least((const void *)kbl_cols<real, L, true>, sm_cols));
         PFAG_TRY(smem_at_least((const void *)kbl_colsE<real, L>, sm_colsE));
@@ -2772,11 +2773,16 @@ struct Fused {
         PFAG_LAUNCHED(c);
         real *X = (real *)r->Y2;              // free once the row pass has read pi_xy: Fx, then the row term
         {
-            const long tasks = (long)Nt * (M / 2);
-            pfag_prof_begin(c, "kbl_rowsD");
-            kbl_rowsD<real, L><<<(unsigned)((tasks + BGm::GPB - 1) / BGm::GPB), BGm::THREADS, sm_rowsD, s>>>(
-                Y1, X, R(c->rho), R(r->Rb), c->dp.dt, c->d_xc, c->d_yc, N, z, M, Nt, tb,
-                c->debug ? R(c->d_vx) : nullptr, c->debug ? R(c->d_vy) : nullptr);
+            const long tasks = (long)Nt * M;
+            pfag_prof_begin(c, "kbl_rowsD1");
+            kbl_rowsD1<real, L><<<(unsigned)((tasks + BGm::GPB - 1) / BGm::GPB), BGm::THREADS, sm_rowsD1, s>>>(
+                Y1, X, R(c->rho), c->d_xc, c->d_yc, N, z, M, Nt, tb, c->debug ? R(c->d_vx) : nullptr,
+                c->debug ? R(c->d_vy) : nullptr);
+            PFAG_LAUNCHED(c);
+            const long pairs = (long)Nt * (M / 2);
+            pfag_prof_begin(c, "kbl_rowsD2");
+            kbl_rowsD2<real, L><<<(unsigned)((pairs + BGm::GPB - 1) / BGm::GPB), BGm::THREADS, sm_rowsD2, s>>>(
+                X, R(r->Rb), c->dp.dt, M, Nt, tb);
             PFAG_LAUNCHED(c);
         }
         {

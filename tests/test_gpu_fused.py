@@ -178,8 +178,8 @@ def test_zone_at_the_ghost_ring():
 
 
 def test_box_not_a_power_of_two():
-    """zone_size 13 gives an FFT box of 24: the fused path's cuFFT-based
-    spectral passes.  Fused FP64 against plain FP64 (fields, areas, velocity)
+    """zone_size 13 gives an FFT box of 24: the fused path's Bluestein
+    spectral passes (inner length 64).  Fused FP64 against plain FP64 (fields, areas, velocity)
     over 3 steps, and the FP32 areas against them."""
     from multicellular_phase_field_active_gel_organoids_b200.params import small_organoid
     cfg = small_organoid(zone_size=13)
@@ -198,8 +198,8 @@ def test_box_not_a_power_of_two():
 
 def test_default_zone_size_200():
     """The reference's default zone_size 200: zones 400 columns wide (a
-    reshaping thread takes several columns) and an FFT box of 398 (cuFFT-based
-    spectral passes), on a 512^2 grid with three cells.  Fused FP64 against
+    reshaping thread takes several columns) and an FFT box of 398 (Bluestein
+    spectral passes, inner length 1024), on a 512^2 grid with three cells.  Fused FP64 against
     plain FP64 over 2 steps, and the FP32 areas against them."""
     from multicellular_phase_field_active_gel_organoids_b200.params import OrganoidConfig
     pts = np.array([(256.0, 256.0), (294.0, 256.0), (237.0, 289.0)])
