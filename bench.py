@@ -235,6 +235,7 @@ def kernel_bytes(cfg, precision: int, iters: dict, ubox: int, uring: int) -> dic
         "kfl_normals": N * N * 8 * w,
         # per launch (two launches per step): read P, Jx, Jy, write Q per active field
         "kl_relax": N * N * 4 * w * (min(lum_it, 2) + min(ecm_it, 2)) // 2,
+        "kl_relax_tma": N * N * 4 * w * (min(lum_it, 2) + min(ecm_it, 2)) // 2,
         # boxes that are not a power of two (Bluestein passes)
         # stresses: reads phi, rho (per cell), lum, ECM (shared); writes Y1 (complex), pi_xy (real), R, class
         "kg_stress": box * (2 * w + 2 * w + w + w + 1) + ubox * 2 * w,

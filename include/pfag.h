@@ -142,6 +142,15 @@ int pfag_seed_organoid(pfag_ctx *ctx, const double *centres, double radius, doub
  * The next step recaptures its graph.  No counterpart in the reference (its
  * OpenACC runtime picks the launch shapes). */
 int pfag_set_launch_shape(pfag_ctx *ctx, int coop_blocks, long update_warps);
+/* Fused path, FP32: tma != 0 runs the lumen / ECM relaxation iterations that
+ * precede the persistent kernel (reshaping_lumen_or_ECM,
+ * cell_phase_functions.cpp:774-869) on tiles staged by TMA (kl_relax_tma)
+ * instead of per-thread copies (kl_relax); the same arithmetic per site, the
+ * rdev tile partials in another grouping.  Off by default: faster alone, but
+ * slower inside the step, where it runs beside the spectral passes.  A knob of
+ * the batched sweep's autotuner.  PFAG_E_UNSUPPORTED unless N_s >= 128 and
+ * N_s % 4 == 0 (FP32 contexts only). */
+int pfag_set_lumen_tiles(pfag_ctx *ctx, int tma);
 
 /* ---- Batches: several organoids (fused-path contexts on the current device)
  * advanced together, the in-process form of the reference's parameter sweep

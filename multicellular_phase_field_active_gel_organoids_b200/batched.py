@@ -21,7 +21,8 @@ cell with a margin of about R), so members share five box sizes and their
 kernel instances (64 and 128 on the register FFTs, 80, 96 and 112 on the
 Bluestein passes).  The autotuner (`autotune`) picks, per bucket of members
 (box size, grid, cell-count class), the launch shapes of the persistent
-relaxation kernel and the phi update (pfag_set_launch_shape) by timing fresh
+relaxation kernel and the phi update (pfag_set_launch_shape), then whether the
+lumen / ECM relaxation runs on TMA-staged tiles (pfag_set_lumen_tiles), by timing fresh
 copies of up to eight of the bucket's members stepped together, and caches the
 choice in a JSON file.
 """
@@ -175,6 +176,8 @@ class BatchedSweep:
             if sh:
                 for i in idx:
                     self.sims[i].set_launch_shape(int(sh["coop_blocks"]), int(sh["update_warps"]))
+                    if sh.get("lumen_tma"):
+                        self.sims[i].set_lumen_tiles(True)
 
     def step(self, it0: int, nsteps: int = 1):
         self.batch.step(it0, nsteps)
@@ -254,10 +257,22 @@ def autotune(members: list[Member], precision: int = 32, cache_path: str | None 
                     t = _time_batch(trial.sims, steps)
                     if best is None or t < best[0]:
                         best = (t, coop, upd)
+                # the lumen / ECM relaxation on TMA-staged tiles, at the best shape
+                tma = 0
+                try:
+                    for sim in trial.sims:
+                        sim.set_launch_shape(best[1], best[2])
+                        sim.set_lumen_tiles(True)
+                except capi.PfagError:
+                    pass                       # not available for this bucket (FP64, small grid)
+                else:
+                    t = _time_batch(trial.sims, steps)
+                    if t < best[0]:
+                        best, tma = (t, best[1], best[2]), 1
             finally:
                 trial.close()
-            cache[ckey] = {"coop_blocks": best[1], "update_warps": best[2], "ms_per_step": round(best[0] * 1e3, 4),
-                           "members_timed": min(sample, len(ms))}
+            cache[ckey] = {"coop_blocks": best[1], "update_warps": best[2], "lumen_tma": tma,
+                           "ms_per_step": round(best[0] * 1e3, 4), "members_timed": min(sample, len(ms))}
         chosen[key] = cache[ckey]
     os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
     with open(path, "w") as f:

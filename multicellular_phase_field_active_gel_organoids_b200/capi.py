@@ -68,6 +68,7 @@ EXPORTS = [
     "pfag_upload_device", "pfag_conv3x3", "pfag_conv3x3_wgrad", "pfag_conv_act_bwd", "pfag_conv_flip", "pfag_adam",
     "pfag_conv_mse", "pfag_corrector_gather", "pfag_corrector_apply",
     "pfag_shard_enable", "pfag_step_head", "pfag_step_tail", "pfag_sum_planes", "pfag_device_field",
+    "pfag_set_lumen_tiles",
 ]
 
 
@@ -105,6 +106,7 @@ def lib() -> ctypes.CDLL:
         L.pfag_launch_count.argtypes = [vp]
         L.pfag_launch_count.restype = ctypes.c_long
         L.pfag_set_launch_shape.argtypes = [vp, ctypes.c_int, ctypes.c_long]
+        L.pfag_set_lumen_tiles.argtypes = [vp, ctypes.c_int]
         L.pfag_seed_organoid.argtypes = [vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong]
         L.pfag_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
         L.pfag_batch_step.argtypes = [vp, ctypes.c_int, ctypes.c_int]
@@ -269,6 +271,10 @@ class Simulation:
 
     def set_launch_shape(self, coop_blocks: int = 0, update_warps: int = 0):
         check(lib().pfag_set_launch_shape(self.h, int(coop_blocks), int(update_warps)))
+
+    def set_lumen_tiles(self, tma: bool):
+        """TMA-staged lumen / ECM relaxation tiles on (True) or off (pfag_set_lumen_tiles)."""
+        check(lib().pfag_set_lumen_tiles(self.h, 1 if tma else 0))
 
     def set_debug(self, flags: int = 1):
         check(lib().pfag_set_debug(self.h, int(flags)))

@@ -173,6 +173,10 @@ int pfag_check_device_error(pfag_ctx *c) {
         return PFAG_E_ZONE;
     }
     if (e & ERRBIT_ITER_CAP) { pfag_set_error("a device relaxation loop hit its iteration cap"); return PFAG_E_RELAX; }
+    if (e & ERRBIT_TIMEOUT) {
+        pfag_set_error("a device wait for a TMA copy gave up after its iteration limit");
+        return PFAG_E_CUDA;
+    }
     if (e & ERRBIT_RELAX) {
         // a cell loop passed rimax: the reference prints and goes on
         // (cell_phase_functions.cpp:563-567); counted, then cleared

@@ -41,6 +41,7 @@ void pfag_fused_free(pfag_ctx *c) {
                     r->part_lt, r->part_a, r->cK, r->G, r->Gsp, r->btw, r->bcw, r->bwf,
                     r->bhdi, r->bh, r->nb_lo};
     for (void *b : bufs) if (b) cudaFree(b);
+    delete r->lmaps;
     delete r;
     c->fused = nullptr;
 }
@@ -62,6 +63,22 @@ extern "C" int pfag_set_launch_shape(pfag_ctx *c, int coop_blocks, long update_w
     r->upd_warps = update_warps > 0 ? update_warps : r->upd_default;
     fused_drop_graph(r);      // the captured step holds the old grid sizes
     r->graph_state = 0;
+    return PFAG_OK;
+}
+
+extern "C" int pfag_set_lumen_tiles(pfag_ctx *c, int tma) {
+    if (!c) { pfag_set_error("null ctx"); return PFAG_E_ARG; }
+    if (c->path != PFAG_PATH_FUSED) { pfag_set_error("the lumen tiles are a fused-path knob"); return PFAG_E_UNSUPPORTED; }
+    FusedRes *r = F(c);
+    if (tma && !r->lmaps) {
+        pfag_set_error("TMA-staged lumen tiles need FP32, N_s >= %d and N_s %% 4 == 0", LT_W);
+        return PFAG_E_UNSUPPORTED;
+    }
+    if (r->lum_tma != (tma != 0)) {
+        r->lum_tma = tma != 0;
+        fused_drop_graph(r);      // the captured step holds the other kernel
+        r->graph_state = 0;
+    }
     return PFAG_OK;
 }
 

@@ -36,6 +36,8 @@
 #include "pfag_regfft.cuh"
 #include "pfag_bluestein.cuh"
 #include <cooperative_groups.h>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -44,6 +46,7 @@
 #include <map>
 #include <type_traits>
 #include <mutex>
+#include <cstring>
 
 namespace cg = cooperative_groups;
 
@@ -66,6 +69,8 @@ inline int smem_at_least(const void *fn, size_t bytes) {
 constexpr int FT = 256;           // threads per block of the fused kernels
 constexpr int RT_I = 8;            // reshaping tile: RT_I zone rows x the full zone width
 
+struct LumMaps;
+
 struct FusedRes {
     void *Y1, *Y2;          // complex [Ntot][M][M]
     void *Rb;               // real [Ntot][M][M]   reaction -deg*rho + gen*P on the box
@@ -86,7 +91,12 @@ struct FusedRes {
     size_t resh_tile;       // one staged strip (3 (RB+2) W reals)
     int ntl;                // lumen/ECM relaxation tiles per field (LRB rows x FT columns)
     size_t lum_tile;        // their staged tile (3 (LRB+2) (FT+2) reals)
-    double *part_lt;        // [2][ntl] tile partial sums
+    double *part_lt;        // [2][max(ntl, ltiles)] tile partial sums
+    LumMaps *lmaps;         // FP32, N >= LT_W, N % 4 == 0: tensor maps of kl_relax_tma (else null)
+    bool lum_tma;           // run the first lumen / ECM iterations as kl_relax_tma (pfag_set_lumen_tiles)
+    int ltiles;             // kl_relax_tma's tiles per field
+    int lt_blocks;          // its persistent grid
+    size_t lt_smem;         // its stages, halo columns and barriers
     // side stream of the lumen/ECM kernels and its fork/join events
     cudaStream_t side;
     cudaEvent_t ev_psi, ev_area, ev_boxA, ev_lum;
@@ -2144,6 +2154,138 @@ __global__ void kl_decide(LumArgs a, int it, const double *__restrict__ part, in
     }
 }
 
+// FP32 lumen / ECM relaxation iteration (the kl_relax step) on tiles of
+// LT_R rows x LT_C columns staged by TMA (cp.async.bulk.tensor 2-D loads of
+// P, J_x, J_y).  A box is LT_W = LT_C + 8 columns wide and starts LT_HX = 4
+// columns left of the tile (a 16-byte aligned x, as TMA requires) and one row
+// above it, so the tile's halo rows and columns come with it; sites outside
+// the grid are zero-filled and feed only the Dirichlet border, which is
+// overwritten.  A persistent block takes the tiles of the active fields in
+// turn with LT_STAGES stages: the next tiles' copies are in flight while it
+// computes one.  Copy completion is an mbarrier with a transaction count;
+// every wait is bounded (ERRBIT_TIMEOUT, and the block drains its other
+// copies before returning).  Tile partials of the rdev sum go to
+// part[f][tile] in tile order, as kl_decide reads them.
+constexpr int LT_R = 16, LT_C = 120, LT_W = 128, LT_HX = 4, LT_THREADS = 128, LT_STAGES = 2;
+constexpr int LT_BOX = (LT_R + 2) * LT_W;                    // floats per plane per stage
+struct LumMaps {
+    CUtensorMap P[4];      // lum, lumn, ECM, ECMn as [N][N] FP32
+    CUtensorMap J[4];      // the lumen / ECM normals: planes 0..3 of Jl
+};
+__device__ __forceinline__ unsigned lt_smem(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ bool lt_wait(unsigned bar, unsigned parity) {
+    for (int k = 0; k < (1 << 20); k++) {
+        unsigned ok;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void lt_load(const CUtensorMap *map, unsigned dst, unsigned bar, int x, int y) {
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+                 ::"r"(dst), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(bar)
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(LT_THREADS) kl_relax_tma(const __grid_constant__ LumMaps maps,
+                                                           float *__restrict__ lum, float *__restrict__ lumn,
+                                                           float *__restrict__ ecm, float *__restrict__ ecmn,
+                                                           LumArgs a, int it, double *__restrict__ part) {
+    extern __shared__ __align__(1024) unsigned char lt_raw[];
+    float *tiles = reinterpret_cast<float *>(lt_raw);                               // [stage][3][LT_R+2][LT_W]
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(tiles + (size_t)LT_STAGES * 3 * LT_BOX);
+    const int N = a.N;
+    const int tj_n = (N + LT_C - 1) / LT_C, tpf = ((N + LT_R - 1) / LT_R) * tj_n;
+    int fl[2], nf = 0;
+    for (int f = 0; f < 2; f++) {
+        const int d = a.done[f];                 // written only by kl_decide, between launches
+        if (!(d != 0 && d < it)) fl[nf++] = f;
+    }
+    const int total = nf * tpf;
+    if ((int)blockIdx.x >= total) return;
+    const int c = threadIdx.x;
+    if (c == 0) {
+        for (int st = 0; st < LT_STAGES; st++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(lt_smem(&bars[st])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    constexpr unsigned BYTES = 3u * LT_BOX * sizeof(float);
+    auto issue = [&](int k) {                    // copies of the block's k-th tile into stage k % LT_STAGES
+        const int t = blockIdx.x + k * gridDim.x;
+        if (t >= total) return;
+        const int f = fl[t / tpf], loc = t - (t / tpf) * tpf;
+        const int ti = loc / tj_n, tj = loc - ti * tj_n;
+        const int st = k % LT_STAGES;
+        const unsigned bar = lt_smem(&bars[st]);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(BYTES) : "memory");
+        float *dst = tiles + (size_t)st * 3 * LT_BOX;
+        const int x = tj * LT_C - LT_HX, y = ti * LT_R - 1;        // x: a multiple of 4 floats
+        lt_load(&maps.P[2 * f + (it & 1)], lt_smem(dst), bar, x, y);
+        lt_load(&maps.J[2 * f], lt_smem(dst + LT_BOX), bar, x, y);
+        lt_load(&maps.J[2 * f + 1], lt_smem(dst + 2 * LT_BOX), bar, x, y);
+    };
+    if (c == 0)
+        for (int k = 0; k < LT_STAGES; k++) issue(k);
+    const ReshConst kc = resh_const(a.A, a.B);
+    const double dx2 = a.dx * a.dx;
+    for (int k = 0;; k++) {
+        const int t = blockIdx.x + k * gridDim.x;
+        if (t >= total) break;
+        const int f = fl[t / tpf], loc = t - (t / tpf) * tpf;
+        const int ti = loc / tj_n, tj = loc - ti * tj_n;
+        const int i0 = ti * LT_R, j0 = tj * LT_C;
+        const int st = k % LT_STAGES;
+        float *Q = (it & 1) ? (f ? ecm : lum) : (f ? ecmn : lumn);
+        const unsigned parity = (unsigned)((k / LT_STAGES) & 1);
+        const bool got = lt_wait(lt_smem(&bars[st]), parity);
+        if (!__syncthreads_and(got)) {            // the same decision in every thread
+            if (c == 0) {
+                atomicOr(a.err, ERRBIT_TIMEOUT);
+                // wait once more (bounded) for this stage's copies and for the
+                // other stages' copies in flight before the block leaves
+                for (int kk = k; kk < k + LT_STAGES; kk++)
+                    if (blockIdx.x + kk * gridDim.x < total)
+                        lt_wait(lt_smem(&bars[kk % LT_STAGES]), (unsigned)((kk / LT_STAGES) & 1));
+            }
+            __syncthreads();
+            return;
+        }
+        // box row rr = tile row + 1, box column = tile column + LT_HX
+        const float *sP = tiles + (size_t)st * 3 * LT_BOX + LT_HX, *sX = sP + LT_BOX, *sY = sX + LT_BOX;
+        const float side_v = f ? 1.0f : 0.0f;
+        const int jj = j0 + c;
+        float facc = 0.0f;
+        if (c < LT_C && jj < N) {
+#pragma unroll 4
+            for (int r = 0; r < LT_R; r++) {
+                const int ii = i0 + r;
+                if (ii >= N) break;
+                const int o = (r + 1) * LT_W + c;
+                float w[3][3];
+#pragma unroll
+                for (int di = 0; di < 3; di++)
+#pragma unroll
+                    for (int dj = 0; dj < 3; dj++) w[di][dj] = sP[o + (di - 1) * LT_W + dj - 1];
+                const float old = w[1][1];
+                const float nv = resh_update_f(kc, w, sX[o], sX[o + LT_W], sX[o - LT_W], sX[o + 1], sX[o - 1], sY[o],
+                                               sY[o + LT_W], sY[o - LT_W], sY[o + 1], sY[o - 1], old);
+                float v;
+                bool edge;
+                dirichlet_val<float>(ii, jj, N, side_v, 0.0f, v, edge);
+                if (!edge) v = nv;
+                facc += fabsf(v - old);
+                Q[(size_t)ii * N + jj] = v;
+            }
+        }
+        const double bs = block_sum_d((double)facc * dx2);    // ends with a block barrier
+        if (c == 0) part[(size_t)f * tpf + loc] = bs;
+        if (c == 0) issue(k + LT_STAGES);         // every thread is past this stage (barrier above)
+    }
+}
+
 // The step ends with lum <- lumn, ECM <- ECMn (run_with_active_gels.cpp:179-181):
 // after an odd iteration count the last iterate already sits in lum / ECM.
 // Copies field f when its count is even and its loop stopped at an iteration
@@ -2286,6 +2428,34 @@ __global__ void kf_rect_init(int4 *rect, int Ntot, int N) {
 // ---------------------------------------------------------------------------
 FusedRes *F(pfag_ctx *c) { return (FusedRes *)c->fused; }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library); null when the driver does not provide it
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        (void)cudaGetLastError();
+    });
+    return fn;
+}
+// [N][N] FP32 plane, boxes of LT_W columns x (LT_R + 2) rows, zero fill outside
+inline bool encode_plane_map(CUtensorMap *m, const void *base, int N) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)N};
+    const cuuint64_t strides[1] = {(cuuint64_t)N * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)LT_W, (cuuint32_t)(LT_R + 2)};
+    const cuuint32_t es[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 BoxArgs box_args(pfag_ctx *c) {
     BoxArgs a{};
     const DevParams &d = c->dp;
@@ -2410,6 +2580,7 @@ struct Fused {
         r->ntl = ((c->N + LRB - 1) / LRB) * ((c->N + FT - 1) / FT);
         r->lum_tile = (size_t)3 * (LRB + 2) * (FT + 2) * sizeof(real);
         PFAG_TRY(smem_at_least((const void *)kl_relax<real>, r->lum_tile));
+        r->ltiles = 0;                 // TMA-staged lumen iterations: set up in alloc, once Jl exists
         r->npsi = ((c->N + 31) / 32) * ((c->N + PT_R - 1) / PT_R);
         r->upd_warps = 0;
         r->upd_smem = (size_t)UPD_SLOTS * 5 * UPD_THREADS * sizeof(float);
@@ -2458,7 +2629,33 @@ struct Fused {
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_r, sizeof(double) * (size_t)c->Ntot * std::max(r->tpc, r->coop_r)));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_e, sizeof(double) * r->npsi));
         PFAG_CUDA_CHECK(cudaMalloc(&r->part_l, sizeof(double) * 2 * r->coop_r));
-        PFAG_CUDA_CHECK(cudaMalloc(&r->part_lt, sizeof(double) * 2 * r->ntl));
+        if (sizeof(real) == 4 && c->N % 4 == 0 && c->N >= LT_W) {
+            // TMA-staged lumen / ECM iterations: the maps hold the addresses of
+            // this context's lum, lumn, ECM, ECMn and of the normals Jl, so
+            // they are encoded after every one of them is allocated
+            LumMaps mp;
+            std::memset(&mp, 0, sizeof(mp));
+            const size_t plane = (size_t)c->N * c->N * sizeof(float);
+            void *pf[4] = {c->lum, c->lumn, c->ecm, c->ecmn};
+            bool ok = r->Jl != nullptr;
+            for (void *q : pf) ok = ok && q != nullptr;
+            for (int k = 0; k < 4 && ok; k++) ok = encode_plane_map(&mp.P[k], pf[k], c->N);
+            for (int k = 0; k < 4 && ok; k++) ok = encode_plane_map(&mp.J[k], (const char *)r->Jl + k * plane, c->N);
+            if (ok) {
+                r->lmaps = new LumMaps(mp);
+                r->ltiles = ((c->N + LT_R - 1) / LT_R) * ((c->N + LT_C - 1) / LT_C);
+                r->lt_smem = (size_t)LT_STAGES * 3 * LT_BOX * sizeof(float) + LT_STAGES * sizeof(long long);
+                PFAG_TRY(smem_at_least((const void *)kl_relax_tma, r->lt_smem));
+                int per = 0;
+                PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kl_relax_tma, LT_THREADS,
+                                                                               r->lt_smem));
+                int dev = 0, nsm = 0;
+                PFAG_CUDA_CHECK(cudaGetDevice(&dev));
+                PFAG_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+                r->lt_blocks = (int)std::min<long>(2L * r->ltiles, (long)nsm * std::max(1, per));
+            }
+        }
+        PFAG_CUDA_CHECK(cudaMalloc(&r->part_lt, sizeof(double) * 2 * std::max(r->ntl, r->ltiles)));
         PFAG_CUDA_CHECK(cudaStreamCreateWithFlags(&r->side, cudaStreamNonBlocking));
         PFAG_CUDA_CHECK(cudaEventCreateWithFlags(&r->ev_psi, cudaEventDisableTiming));
         PFAG_CUDA_CHECK(cudaEventCreateWithFlags(&r->ev_boxA, cudaEventDisableTiming));
@@ -2643,6 +2840,18 @@ struct Fused {
         //    after the join below
         if (fork) PFAG_CUDA_CHECK(cudaStreamWaitEvent(s2, r->ev_boxA, 0));
         for (int it = 1; it <= LUM_REGULAR; it++) {
+            if constexpr (sizeof(real) == 4) {
+                if (r->lmaps && r->lum_tma) {
+                    pfag_prof_begin(c, "kl_relax_tma");
+                    kl_relax_tma<<<r->lt_blocks, LT_THREADS, r->lt_smem, s2>>>(
+                        *r->lmaps, R(c->lum), R(c->lumn), R(c->ecm), R(c->ecmn), la, it, r->part_lt);
+                    PFAG_LAUNCHED(c);
+                    pfag_prof_begin(c, "kl_decide");
+                    kl_decide<<<2, 32, 0, s2>>>(la, it, r->part_lt, r->ltiles);
+                    PFAG_LAUNCHED(c);
+                    continue;
+                }
+            }
             pfag_prof_begin(c, "kl_relax");
             kl_relax<real><<<dim3(r->ntl, 2), FT, r->lum_tile, s2>>>(R(c->lum), R(c->lumn), R(c->ecm), R(c->ecmn),
                                                                       R(r->Jl), la, it, r->part_lt);

@@ -41,6 +41,7 @@ enum : unsigned {
     ERRBIT_ZONE = 2u,
     ERRBIT_RELAX = 4u,
     ERRBIT_ITER_CAP = 8u,
+    ERRBIT_TIMEOUT = 16u,     // a bounded device wait (a TMA copy's completion) gave up
 };
 
 // Scalars the kernels read, precomputed on the host in double with the

@@ -96,6 +96,7 @@ def test_autotune_writes_cache(tmp_path):
     for key, sh in shapes.items():
         assert cache[f"{key}_fp32"] == sh
         assert (sh["coop_blocks"], sh["update_warps"]) in B.SHAPES
+        assert sh["lumen_tma"] in (0, 1)             # the 256^2 members can take TMA lumen tiles
     with B.BatchedSweep(ms, precision=32) as sw:
         sw.set_shapes(shapes)
         sw.step(0, 3)

@@ -60,6 +60,39 @@ def test_fused_fp32_tiny_area(tiny_ref):
     assert rel_linf(got["s"], ref["s"]) <= 1e-4
 
 
+def test_fp32_lumen_relaxation_on_tma_tiles():
+    """cfg0 (256^2) with the FP32 lumen / ECM relaxation on TMA-staged tiles
+    (pfag_set_lumen_tiles, kl_relax_tma) over 5 steps (the first eager, the
+    rest graph replays): the same iteration counts as with the per-thread
+    copies and the same fields to FP32 rounding (the same formula per site,
+    compiled in another kernel), and within FP32 of the plain FP64 path; the
+    knob is refused on a grid too small for the tiles."""
+    cfg = CONFIGS["cfg0"]()
+    init = cfg.initial_state(np.float32)
+    out = {}
+    for tma in (False, True):
+        with capi.Simulation(cfg.params(), 32, capi.PATH_FUSED) as sim:
+            sim.set_relax_cap(100000)
+            sim.set_lumen_tiles(tma)
+            sim.upload(*init)
+            sim.step(0, 5)
+            out[tma] = (sim.download(), sim.stats())
+    (fa, sa), (fb, sb) = out[False], out[True]
+    assert (sa["lum_iters"], sa["ecm_iters"]) == (sb["lum_iters"], sb["ecm_iters"])
+    for k, x, y in zip(("phi", "rho", "lum", "ECM"), fa, fb):
+        d = float(np.abs(x.astype(np.float64) - y).max())
+        print("tma vs copies", k, d)
+        assert d <= 1e-5, (k, d)
+    b = run_gpu(cfg, 5, 64, capi.PATH_PLAIN)
+    assert (sb["lum_iters"], sb["ecm_iters"]) == (b["stats"]["lum_iters"], b["stats"]["ecm_iters"])
+    for k, x in zip(("lum", "ECM"), fb[2:]):
+        assert np.abs(x - b[k]).max() <= 1e-5, (k, np.abs(x - b[k]).max())
+    tiny = CONFIGS["tiny"]()
+    with capi.Simulation(tiny.params(), 32, capi.PATH_FUSED) as sim:
+        with pytest.raises(capi.PfagError):
+            sim.set_lumen_tiles(True)
+
+
 def test_fused_vs_plain_cfg0_fp64():
     cfg = CONFIGS["cfg0"]()
     a = run_gpu(cfg, 4, 64, capi.PATH_FUSED)
