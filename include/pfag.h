@@ -105,7 +105,12 @@ int pfag_get_stats(pfag_ctx *ctx, pfag_stats *st);
 int pfag_get_cell_iters(pfag_ctx *ctx, int *iters);
 /* Per-cell velocity of the last step's spectral solve, Re(IFFT(v))/M^2 on the
  * FFT box (rho_functions.cpp:449-456): vx, vy [Ntot][M][M], M = 2*zone_size-2.
- * Requires pfag_set_debug(ctx, 1) before the step. */
+ * Requires pfag_set_debug(ctx, 1) before the step.  Any nonzero flags keep
+ * the fused path eager (no graph).  Bit 2 (flags & 2) is a test hook of the
+ * device-side wait limits: the TMA-staged lumen tiles (pfag_set_lumen_tiles)
+ * then wait for copies that are never issued, so their bounded waits run out
+ * with nothing in flight; the next synchronising call returns PFAG_E_CUDA
+ * once ("a device wait ... gave up") and the context stays usable. */
 int pfag_set_debug(pfag_ctx *ctx, int flags);
 int pfag_get_velocity(pfag_ctx *ctx, void *vx, void *vy);
 

@@ -172,11 +172,14 @@ int pfag_check_device_error(pfag_ctx *c) {
         pfag_set_error("a cell's zone [xc-%d, xc+%d) leaves the grid interior", c->zone, c->zone);
         return PFAG_E_ZONE;
     }
-    if (e & ERRBIT_ITER_CAP) { pfag_set_error("a device relaxation loop hit its iteration cap"); return PFAG_E_RELAX; }
     if (e & ERRBIT_TIMEOUT) {
+        // reported once and cleared: the kernel returned, the context stays usable
         pfag_set_error("a device wait for a TMA copy gave up after its iteration limit");
+        PFAG_CUDA_CHECK(cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), c->stream));
+        PFAG_CUDA_CHECK(cudaStreamSynchronize(c->stream));
         return PFAG_E_CUDA;
     }
+    if (e & ERRBIT_ITER_CAP) { pfag_set_error("a device relaxation loop hit its iteration cap"); return PFAG_E_RELAX; }
     if (e & ERRBIT_RELAX) {
         // a cell loop passed rimax: the reference prints and goes on
         // (cell_phase_functions.cpp:563-567); counted, then cleared

@@ -1843,6 +1843,9 @@ struct LumArgs {
     double *part;      // [2][gridDim]
     int *K, *done, *cnt;
     unsigned *err;
+    int no_copies;     // kl_relax_tma test hook: expect each stage's bytes but issue no copy, so no
+                       // stage completes and the bounded waits run out (nothing in flight when they do)
+    int wait_cap;      // kl_relax_tma: try_wait attempts per wait before it gives up
 };
 
 template <typename real>
@@ -2173,8 +2176,8 @@ struct LumMaps {
     CUtensorMap J[4];      // the lumen / ECM normals: planes 0..3 of Jl
 };
 __device__ __forceinline__ unsigned lt_smem(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ bool lt_wait(unsigned bar, unsigned parity) {
-    for (int k = 0; k < (1 << 20); k++) {
+__device__ __forceinline__ bool lt_wait(unsigned bar, unsigned parity, int cap) {
+    for (int k = 0; k < cap; k++) {
         unsigned ok;
         asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
                      " selp.u32 %0, 1, 0, p;\n}\n"
@@ -2221,6 +2224,7 @@ __global__ void __launch_bounds__(LT_THREADS) kl_relax_tma(const __grid_constant
         const int st = k % LT_STAGES;
         const unsigned bar = lt_smem(&bars[st]);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(BYTES) : "memory");
+        if (a.no_copies) return;
         float *dst = tiles + (size_t)st * 3 * LT_BOX;
         const int x = tj * LT_C - LT_HX, y = ti * LT_R - 1;        // x: a multiple of 4 floats
         lt_load(&maps.P[2 * f + (it & 1)], lt_smem(dst), bar, x, y);
@@ -2240,7 +2244,7 @@ __global__ void __launch_bounds__(LT_THREADS) kl_relax_tma(const __grid_constant
         const int st = k % LT_STAGES;
         float *Q = (it & 1) ? (f ? ecm : lum) : (f ? ecmn : lumn);
         const unsigned parity = (unsigned)((k / LT_STAGES) & 1);
-        const bool got = lt_wait(lt_smem(&bars[st]), parity);
+        const bool got = lt_wait(lt_smem(&bars[st]), parity, a.wait_cap);
         if (!__syncthreads_and(got)) {            // the same decision in every thread
             if (c == 0) {
                 atomicOr(a.err, ERRBIT_TIMEOUT);
@@ -2248,7 +2252,7 @@ __global__ void __launch_bounds__(LT_THREADS) kl_relax_tma(const __grid_constant
                 // other stages' copies in flight before the block leaves
                 for (int kk = k; kk < k + LT_STAGES; kk++)
                     if (blockIdx.x + kk * gridDim.x < total)
-                        lt_wait(lt_smem(&bars[kk % LT_STAGES]), (unsigned)((kk / LT_STAGES) & 1));
+                        lt_wait(lt_smem(&bars[kk % LT_STAGES]), (unsigned)((kk / LT_STAGES) & 1), a.wait_cap);
             }
             __syncthreads();
             return;
@@ -2787,6 +2791,8 @@ struct Fused {
         la.A = d.A_resh; la.B = d.B_resh; la.thr = d.thr_lum; la.rdev0 = d.rdev0_lum;
         la.part_e = r->part_e; la.part = r->part_l; la.K = r->lK; la.done = r->ldone; la.cnt = r->lcnt;
         la.err = c->d_err;
+        la.no_copies = (c->debug & 2) ? 1 : 0;               // pfag_set_debug bit 2: the TMA waits run out
+        la.wait_cap = (c->debug & 2) ? (1 << 10) : (1 << 20);
         {
             pfag_prof_begin(c, "kfl_sum_ecm");
             kfl_sum_ecm<<<1, 32, 0, s2>>>(r->part_e, r->npsi, c->d_scal + 0);

@@ -93,6 +93,30 @@ def test_fp32_lumen_relaxation_on_tma_tiles():
             sim.set_lumen_tiles(True)
 
 
+def test_tma_wait_limit_reports_and_recovers():
+    """The bounded waits of the TMA-staged lumen tiles: with the copies not
+    issued (pfag_set_debug bit 2, a host-side switch: nothing is in flight)
+    no stage completes, every wait gives up after its limit, the step
+    reports PFAG_E_CUDA once, and the context steps normally again (no fault,
+    no hang: the kernel returns)."""
+    cfg = CONFIGS["cfg0"]()
+    init = cfg.initial_state(np.float32)
+    with capi.Simulation(cfg.params(), 32, capi.PATH_FUSED) as sim:
+        sim.set_lumen_tiles(True)
+        sim.upload(*init)
+        sim.set_debug(2)
+        with pytest.raises(capi.PfagError) as e:
+            sim.step(0, 1)
+        assert e.value.code == -2 and "gave up" in str(e.value)
+        sim.set_debug(0)
+        sim.set_relax_cap(100000)
+        sim.upload(*init)
+        sim.step(0, 3)
+        phi, rho, lum, ecm = sim.download()
+    ref = run_gpu(cfg, 3, 32, capi.PATH_FUSED)
+    assert np.abs(lum - ref["lum"]).max() <= 1e-5 and np.abs(phi - ref["phi"]).max() <= 1e-5
+
+
 def test_fused_vs_plain_cfg0_fp64():
     cfg = CONFIGS["cfg0"]()
     a = run_gpu(cfg, 4, 64, capi.PATH_FUSED)
