@@ -2196,8 +2196,12 @@ __global__ void __launch_bounds__(LT_THREADS) kl_relax_tma(const __grid_constant
                                                            float *__restrict__ lum, float *__restrict__ lumn,
                                                            float *__restrict__ ecm, float *__restrict__ ecmn,
                                                            LumArgs a, int it, double *__restrict__ part) {
-    extern __shared__ __align__(1024) unsigned char lt_raw[];
-    float *tiles = reinterpret_cast<float *>(lt_raw);                               // [stage][3][LT_R+2][LT_W]
+    // TMA destinations 128-byte aligned (the dynamic allocation has 128 bytes
+    // of slack for it; an aligned extern declaration would pad every kernel's
+    // shared memory in this file)
+    extern __shared__ unsigned char lt_raw[];
+    float *tiles = reinterpret_cast<float *>(
+        lt_raw + ((128u - (lt_smem(lt_raw) & 127u)) & 127u));                      // [stage][3][LT_R+2][LT_W]
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(tiles + (size_t)LT_STAGES * 3 * LT_BOX);
     const int N = a.N;
     const int tj_n = (N + LT_C - 1) / LT_C, tpf = ((N + LT_R - 1) / LT_R) * tj_n;
@@ -2648,7 +2652,7 @@ struct Fused {
             if (ok) {
                 r->lmaps = new LumMaps(mp);
                 r->ltiles = ((c->N + LT_R - 1) / LT_R) * ((c->N + LT_C - 1) / LT_C);
-                r->lt_smem = (size_t)LT_STAGES * 3 * LT_BOX * sizeof(float) + LT_STAGES * sizeof(long long);
+                r->lt_smem = (size_t)LT_STAGES * 3 * LT_BOX * sizeof(float) + LT_STAGES * sizeof(long long) + 128;
                 PFAG_TRY(smem_at_least((const void *)kl_relax_tma, r->lt_smem));
                 int per = 0;
                 PFAG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kl_relax_tma, LT_THREADS,
