@@ -56,6 +56,32 @@ def test_one_cell_per_shard_matches_reference():
         _check_against(ref, sh)
 
 
+def test_shards_on_bluestein_boxes():
+    """The reference's default zone_size 200 (FFT box 398: the Bluestein
+    passes, whose stress kernel reads the neighbour planes) on a 512^2 grid
+    with three cells, one per shard: FP64 against the unsharded fused step
+    after 2 steps (psi summed in another grouping: rounding only)."""
+    from multicellular_phase_field_active_gel_organoids_b200.params import OrganoidConfig
+    pts = np.array([(256.0, 256.0), (294.0, 256.0), (237.0, 289.0)])
+    cfg = OrganoidConfig("wide", 512, pts, 20.0, 200, 0, 2)
+    init = cfg.initial_state(np.float64)
+    with capi.Simulation(cfg.params(), 64, capi.PATH_FUSED) as s:
+        s.set_relax_cap(100000)
+        s.upload(*init)
+        s.step(0, 2)
+        one = s.download()
+        a1 = s.areas()[0]
+        c1 = s.centres()
+    with sharded.LocalShards(cfg.params(), init, 3, precision=64, relax_cap=100000) as sh:
+        sh.step(0, 2)
+        got = sh.download()
+        assert rel(sh.areas(), a1) <= 1e-12
+        xc, yc = sh.centres()
+    assert np.array_equal(xc, c1[0]) and np.array_equal(yc, c1[1])
+    for a, b in zip(got, one):
+        assert rel(a, b) <= 1e-12
+
+
 def test_shards_fp32_close_to_unsharded():
     """FP32: psi summed per shard then over shards rounds differently from one running sum."""
     cfg = hex_ring_organoid()
