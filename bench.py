@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--members", type=int, default=256, help="cfg3: organoids in the batched sweep")
     ap.add_argument("--no-tune", action="store_true", help="cfg3: default launch shapes (no autotuning)")
     ap.add_argument("--pairs", type=int, default=32, help="cfg4: coarse/fine training pairs")
+    ap.add_argument("--lumen-tma", action="store_true",
+                    help="run the first lumen/ECM relaxation iterations on TMA-staged tiles (pfag_set_lumen_tiles)")
     ap.add_argument("--shard", action="store_true",
                     help="split one organoid's cells over the ranks (psi all-reduce, neighbour halo): strong scaling")
     return ap.parse_args()
@@ -294,6 +296,8 @@ def run_ours(args, ws, rank, local, dist: Dist):
     rt.cudaStreamSynchronize.argtypes = [ctypes.c_void_p]
 
     sim = capi.Simulation(p, prec, capi.PATH_FUSED)
+    if args.lumen_tma:
+        sim.set_lumen_tiles(True)
     sim.upload(*init)
     stream = ctypes.c_void_p(sim.stream())
     nev = args.steps
@@ -419,6 +423,8 @@ def run_e2e(args, cfg, p, prec, init, rt, capi, sites, dist):
     for a in obs:
         rt.cudaHostRegister(a.ctypes.data, a.nbytes, 0)
     sim = capi.Simulation(p, prec, capi.PATH_FUSED)
+    if args.lumen_tma:
+        sim.set_lumen_tiles(True)
     L = capi.lib()
     dist.barrier()
     t0 = time.perf_counter()
@@ -660,7 +666,8 @@ def main():
             "data": "synthetic (seeded organoid inputs generated in-process; no dataset)",
             "config": dict(config, path="fused", precision=("f32 with f64 areas/loop sums" if args.precision == 32
                                                             else "f64"),
-                           parallelism=f"replicas x{ws}"),
+                           parallelism=f"replicas x{ws}",
+                           lumen_tiles="TMA-staged" if args.lumen_tma else "per-thread copies"),
             "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"],
             "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
             "active_site_updates_per_s": res["value"] * (2 * cfg.zone_size) ** 2 / cfg.N ** 2,
