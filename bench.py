@@ -238,6 +238,14 @@ def kernel_bytes(cfg, precision: int, iters: dict, ubox: int, uring: int) -> dic
         # per launch (two launches per step): read P, Jx, Jy, write Q per active field
         "kl_relax": N * N * 4 * w * (min(lum_it, 2) + min(ecm_it, 2)) // 2,
         "kl_relax_tma": N * N * 4 * w * (min(lum_it, 2) + min(ecm_it, 2)) // 2,
+        # power-of-two boxes of 16, 512 or 1024 (shared-memory radix-4 passes): A as kr_boxA; B reads both
+        # row spectra and the class map, writes the velocity spectrum; C reads it and rho, writes the
+        # fluxes' spectrum; D transforms it back along the columns; E reads it, rho and R, writes rho
+        "kf_boxA": box * (2 * w + 2 * w + 2 * w + w + 1) + ubox * 2 * w,
+        "kf_boxB": box * (2 * w + 2 * w + 1 + 2 * w),
+        "kf_boxC": box * (2 * w + w + 2 * w),
+        "kf_boxD": box * 4 * w,
+        "kf_boxE": box * (2 * w + w + w + w),
         # boxes that are not a power of two (Bluestein passes)
         # stresses: reads phi, rho (per cell), lum, ECM (shared); writes Y1 (complex), pi_xy (real), R, class
         "kg_stress": box * (2 * w + 2 * w + w + w + 1) + ubox * 2 * w,
